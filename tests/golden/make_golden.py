@@ -1,0 +1,396 @@
+"""Generate golden vectors by running the reference implementation itself.
+
+Run in a container that has the reference checked out (read-only) at
+``$GMF_REFERENCE`` (default ``/root/reference``)::
+
+    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py
+
+It imports ``graphmambaformer.alignment`` from the reference, feeds it seeded
+synthetic inputs, and stores inputs + outputs as small compressed ``.npz``
+fixtures next to this script.  The GPU test suite and the oracle tests read
+only these fixtures; nothing at test time imports the reference.
+
+Fixtures:
+
+* ``sw_golden.npz``     -- ``banded_affine_sw_batch`` (B=1 per pair) +
+  ``traceback_banded``: the reference's known-answer pairs
+  (tests/test_accel.py L306-334, tests/test_alignment_stages.py L1029-1048),
+  edge cases (empty query, band outside the target, N bases, negative
+  offsets, x-drop cut-offs, half band 0) and seeded random pairs.
+* ``chain_golden.npz``  -- ``chain_dp_numpy`` on random inputs (with and
+  without a bonus, several lookbacks) including the known-answer anchors of
+  tests/test_accel.py L347-370, plus ``AffineChainer.chain`` on minimizer
+  anchors of simulated HiFi reads.
+* ``extend_golden.npz`` -- ``ExtensionEngine.extend_chains`` on single-chain
+  calls (window, band widening, soft clips).
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+REF = os.environ.get("GMF_REFERENCE", "/root/reference")
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))  # repo root
+sys.path.insert(0, REF)
+sys.dont_write_bytecode = True
+
+import torch  # noqa: E402
+
+torch.set_num_threads(1)
+
+from graphmambaformer.alignment.chaining import AffineChainer, chain_dp_numpy  # noqa: E402
+from graphmambaformer.alignment.extension import (  # noqa: E402
+    ExtensionEngine,
+    banded_affine_sw_batch,
+    traceback_banded,
+)
+from graphmambaformer.alignment.seeding import encode_bases  # noqa: E402
+from graphmambaformer.alignment.types import AnchorSet, Chain  # noqa: E402
+from graphmambaformer.config import ChainingConfig, ExtensionConfig  # noqa: E402
+
+from graphmambaformer_b200 import synth  # noqa: E402
+
+OPS = "=XIDS"
+
+
+def cigar_words(cigar):
+    return np.array([(n << 4) | OPS.index(op) for op, n in cigar], dtype=np.uint32)
+
+
+def ragged(arrs, dtype):
+    off = np.zeros(len(arrs) + 1, dtype=np.int64)
+    np.cumsum([len(a) for a in arrs], out=off[1:])
+    flat = np.concatenate([np.asarray(a, dtype=dtype) for a in arrs]) if off[-1] else np.zeros(0, dtype)
+    return flat, off
+
+
+# --------------------------------------------------------------------------- #
+# Banded SW
+# --------------------------------------------------------------------------- #
+def sw_case(q, t, hb, off, params):
+    cfg = ExtensionConfig(match_score=params[0], mismatch_penalty=params[1],
+                          gap_open=params[2], gap_extend=params[3], x_drop=params[4])
+    qt = torch.as_tensor(np.asarray(q, dtype=np.int16))[None]
+    tt = torch.as_tensor(np.asarray(t, dtype=np.int16))[None]
+    res = banded_affine_sw_batch(qt, tt, torch.tensor([len(q)]), torch.tensor([len(t)]), cfg,
+                                 half_band=hb, band_offset=torch.tensor([off]),
+                                 return_matrices=True)
+    ext = traceback_banded(res, 0, np.asarray(q), np.asarray(t), cfg)
+    return dict(score=float(res.score[0]), qe=int(res.query_end[0]), te=int(res.target_end[0]),
+                qs=int(ext.read_start), ts=int(ext.ref_start), cigar=cigar_words(ext.cigar),
+                counts=[ext.n_match, ext.n_mismatch, ext.n_insertion, ext.n_deletion])
+
+
+def make_sw(rng):
+    cases = []  # (q, t, hb, off, params, tag)
+    default = (2.0, 4.0, 6.0, 2.0, 600.0)
+    cfg1 = (2.0, 4.0, 4.0, 2.0, 0.0)
+    # known answers from the reference's own tests
+    cases.append((encode_bases("ACGT"), encode_bases("TTACGTAA"), 2, 2, default, "ka_acgt"))
+    s40 = "".join(rng.choice(list("ACGT"), size=40))
+    cases.append((encode_bases(s40), encode_bases(s40), 8, 0, default, "ka_identical40"))
+    # edge cases
+    r = lambda n: rng.integers(1, 5, size=n).astype(np.int8)  # noqa: E731
+    cases.append((np.zeros(0, np.int8), r(10), 3, 0, default, "empty_query"))
+    cases.append((r(1), r(1), 0, 0, default, "one_base_hb0"))
+    x = r(30)
+    cases.append((x, x.copy(), 0, 0, default, "hb0_identical"))
+    cases.append((r(20), r(20), 5, 40, default, "band_right_of_target"))
+    cases.append((r(20), r(20), 5, -40, default, "band_left_of_target"))
+    y = r(50)
+    cases.append((y[5:45], y, 4, -3, default, "negative_offset"))
+    yn = y.copy()
+    yn[[3, 10, 22]] = 5
+    cases.append((yn, y, 6, 0, default, "query_N"))
+    cases.append((y, yn, 6, 0, default, "target_N"))
+    cases.append((yn, yn.copy(), 6, 0, default, "both_N"))
+    cases.append((r(25), r(60), 40, 10, default, "band_wider_than_target"))
+    # x-drop: a matching prefix followed by random sequence
+    base = r(200)
+    qx = np.concatenate([base[:80], r(120)])
+    for xd in (5.0, 10.0, 20.0, 40.0):
+        cases.append((qx, base, 10, 0, (2.0, 4.0, 6.0, 2.0, xd), f"xdrop_{int(xd)}"))
+    # gap-heavy pairs: insertions and deletions of several lengths
+    for L in (1, 2, 3, 5, 8):
+        t0 = r(120)
+        q_ins = np.concatenate([t0[:60], r(L), t0[60:]])
+        q_del = np.concatenate([t0[:60], t0[60 + L:]])
+        cases.append((q_ins, t0, 12, 0, default, f"ins_{L}"))
+        cases.append((q_del, t0, 12, 0, default, f"del_{L}"))
+        cases.append((q_ins, t0, 12, 0, cfg1, f"ins_{L}_cfg1"))
+        cases.append((q_del, t0, 12, 0, cfg1, f"del_{L}_cfg1"))
+    # exhaustive-ish tiny cases: every small band / offset / length combination
+    for hb in (0, 1, 2, 3):
+        for off in range(-3, 6):
+            for ql in (1, 2, 4, 7):
+                for tl in (1, 3, 6, 9):
+                    cases.append((r(ql), r(tl), hb, off, default, "tiny"))
+    # random scoring parameters (integers, including open < extend)
+    for k in range(40):
+        ql = int(rng.integers(5, 60))
+        t0 = r(ql + int(rng.integers(0, 20)))
+        q0 = synth.apply_errors(t0[: ql], synth.ONT, rng)
+        params = (float(rng.integers(1, 5)), float(rng.integers(1, 7)), float(rng.integers(0, 9)),
+                  float(rng.integers(0, 5)), float(rng.choice([0, 0, 7, 15, 600])))
+        cases.append((q0, t0, int(rng.integers(0, 12)), int(rng.integers(-5, 10)), params, "randparams"))
+    # the 150 bp extension workload, first 150 pairs
+    ps = synth.extension_pairs_150bp(n_pairs=150, seed=11, ref_len=200_000)
+    for b in range(len(ps)):
+        cases.append((ps.q(b), ps.t(b), 32, 32, cfg1, "cfg1"))
+    # mixed-profile medium pairs with widened bands
+    mixed = synth.extension_pairs_mixed(n_pairs=24, seed=5, ref_len=400_000, max_len=1500,
+                                        log_mean=6.0, log_sigma=0.6)
+    for b in range(len(mixed)):
+        cases.append((mixed.q(b), mixed.t(b), int(mixed.half_band[b]), 32, default, "mixed"))
+    out = [sw_case(q, t, hb, off, p) for (q, t, hb, off, p, _) in cases]
+    q_flat, q_off = ragged([c[0] for c in cases], np.int8)
+    t_flat, t_off = ragged([c[1] for c in cases], np.int8)
+    cg_flat, cg_off = ragged([o["cigar"] for o in out], np.uint32)
+    np.savez_compressed(
+        os.path.join(HERE, "sw_golden.npz"),
+        query=q_flat, query_off=q_off, target=t_flat, target_off=t_off,
+        half_band=np.array([c[2] for c in cases], np.int32),
+        band_offset=np.array([c[3] for c in cases], np.int32),
+        params=np.array([c[4] for c in cases], np.float64),
+        tag=np.array([c[5] for c in cases]),
+        score=np.array([o["score"] for o in out], np.float32),
+        query_end=np.array([o["qe"] for o in out], np.int64),
+        target_end=np.array([o["te"] for o in out], np.int64),
+        query_start=np.array([o["qs"] for o in out], np.int64),
+        target_start=np.array([o["ts"] for o in out], np.int64),
+        counts=np.array([o["counts"] for o in out], np.int64),
+        cigar=cg_flat, cigar_off=cg_off,
+    )
+    print(f"sw_golden.npz: {len(cases)} pairs")
+
+
+# --------------------------------------------------------------------------- #
+# Chaining
+# --------------------------------------------------------------------------- #
+def lut_for(cfg: ChainingConfig) -> np.ndarray:
+    gap = np.arange(cfg.max_gap + 1, dtype=np.int64)
+    return np.where(gap > 0, cfg.gap_open + cfg.gap_extend * gap + cfg.log_coeff * np.log2(gap + 1.0), 0.0)
+
+
+def chimeric_batch(rng, n_reads=10):
+    """Reads stitched from 2-3 segments (either strand) of a reference that
+    also carries a diverged copy of one region, so reads have several chains
+    on both strands, secondary candidates and overlapping repeats."""
+    ref = synth.random_reference(600_000, rng)
+    src = ref[100_000:104_000].copy()
+    dup = synth.apply_errors(src, synth.ErrorProfile(0.01, 0.0, 0.0), rng)[:4000]
+    ref[400_000:400_000 + len(dup)] = dup
+    sketch = synth.MinimizerSketch(ref, k=15, w=10)
+    rp, fp, ln, st, counts, rl = [], [], [], [], [], []
+    for r in range(n_reads):
+        parts = []
+        for s in range(int(rng.integers(2, 4))):
+            L = int(rng.integers(600, 2500))
+            if r % 3 == 0 and s == 0:
+                start = 100_000 + int(rng.integers(0, 1000))  # lands in the repeat
+            else:
+                start = int(rng.integers(0, len(ref) - L))
+            seg = ref[start:start + L]
+            if rng.random() < 0.5:
+                seg = synth.reverse_complement(seg)
+            parts.append(synth.apply_errors(seg, synth.HIFI, rng))
+        read = np.concatenate(parts)
+        n = 0
+        for strand, codes in ((1, read), (-1, synth.reverse_complement(read))):
+            a, b = sketch.query(codes)
+            rp.append(a); fp.append(b)
+            ln.append(np.full(len(a), 15, np.int64)); st.append(np.full(len(a), strand, np.int8))
+            n += len(a)
+        counts.append(n)
+        rl.append(len(read))
+    off = np.zeros(n_reads + 1, np.int64)
+    np.cumsum(counts, out=off[1:])
+    return synth.AnchorBatch(off, np.concatenate(rp).astype(np.int32), np.concatenate(fp).astype(np.int32),
+                             np.concatenate(ln).astype(np.int32), np.concatenate(st).astype(np.int8),
+                             np.array(rl, np.int64))
+
+
+def group_batch(rng, n_reads=8):
+    """Hand-built anchor sets: many collinear groups with distinct or
+    overlapping read spans and random strands, to exercise the score cutoff,
+    the overlap filter and the max_chains cap of select()."""
+    rp, fp, ln, st, counts = [], [], [], [], []
+    for r in range(n_reads):
+        n_groups = int(rng.integers(3, 14))
+        n = 0
+        for g in range(n_groups):
+            k = int(rng.integers(2, 40))
+            start = int(rng.integers(0, 20_000)) if r % 2 else g * 1500
+            diag = int(rng.integers(0, 5_000_000))
+            pos = start + np.cumsum(rng.integers(10, 40, size=k))
+            drift = np.cumsum(rng.integers(-2, 3, size=k)) if r % 4 == 3 else 0
+            rp.append(pos)
+            fp.append(pos + diag + drift)
+            ln.append(rng.integers(12, 25, size=k))
+            st.append(np.full(k, 1 if rng.random() < 0.6 else -1, np.int8))
+            n += k
+        counts.append(n)
+    off = np.zeros(n_reads + 1, np.int64)
+    np.cumsum(counts, out=off[1:])
+    return synth.AnchorBatch(off, np.concatenate(rp).astype(np.int32), np.concatenate(fp).astype(np.int32),
+                             np.concatenate(ln).astype(np.int32), np.concatenate(st).astype(np.int8),
+                             np.full(n_reads, 30_000, np.int64))
+
+
+def make_chain(rng):
+    # --- DP level ---
+    dp_cases = []  # (read_end, ref_end, weight, bonus or None, lookback, max_gap)
+    dp_cases.append((np.array([10, 20, 30]), np.array([10, 20, 31]), np.array([10.5, 9.25, 8.75]),
+                     None, 64, 5000))
+    for trial in range(40):
+        n = int(rng.integers(1, 120))
+        re = np.sort(rng.integers(1, 2000, size=n)).astype(np.int64)
+        fe = np.sort(rng.integers(1, 2000, size=n)).astype(np.int64)
+        w = rng.integers(5, 40, size=n).astype(np.float64)
+        if trial % 3 == 0:
+            w = w + rng.random(n)  # fractional weights (hybrid gate)
+        lb = int(rng.choice([1, 4, 16, 50, 64, 200]))
+        mg = int(rng.choice([100, 500, 5000]))
+        bonus = None
+        if trial % 4 == 1:
+            bonus = rng.normal(0, 3, size=(n, lb))
+        dp_cases.append((re, fe, w, bonus, lb, mg))
+    # ties: equal scores from several predecessors (collinear grid)
+    re = np.repeat(np.arange(1, 21) * 10, 1)
+    dp_cases.append((re, re.copy(), np.full(20, 15.0), None, 8, 5000))
+    grid = np.array([10, 10, 20, 20, 30, 30, 40, 40])
+    dp_cases.append((grid, np.array([10, 12, 20, 22, 30, 32, 40, 42]), np.full(8, 12.0), None, 4, 5000))
+    f_all, p_all = [], []
+    for (re, fe, w, bonus, lb, mg) in dp_cases:
+        cfg = ChainingConfig(max_lookback=lb, max_gap=mg)
+        f, p = chain_dp_numpy(re, fe, w, cfg, bonus=bonus)
+        f_all.append(f)
+        p_all.append(p)
+    re_flat, dp_off = ragged([c[0] for c in dp_cases], np.int64)
+    fe_flat, _ = ragged([c[1] for c in dp_cases], np.int64)
+    w_flat, _ = ragged([c[2] for c in dp_cases], np.float64)
+    has_bonus = np.array([c[3] is not None for c in dp_cases])
+    bonus_flat, bonus_off = ragged([np.asarray(c[3]).ravel() if c[3] is not None else np.zeros(0)
+                                    for c in dp_cases], np.float64)
+    f_flat, _ = ragged(f_all, np.float64)
+    p_flat, _ = ragged(p_all, np.int64)
+
+    # --- chain() level on simulated minimizer anchors ---
+    batches = [
+        synth.chaining_reads_hifi(n_reads=24, seed=21, ref_len=1_000_000, mean_len=3000),
+        synth.chaining_reads_hifi(n_reads=4, seed=22, ref_len=2_000_000, mean_len=15_000),
+        synth.chaining_reads_hifi(n_reads=6, seed=23, ref_len=500_000, mean_len=4000,
+                                  profile=synth.ONT),
+    ]
+    lookbacks = [50, 50, 200]
+    batches.append(chimeric_batch(rng))
+    lookbacks.append(50)
+    batches.append(group_batch(rng))
+    lookbacks.append(64)
+    reads_rp, reads_fp, reads_ln, reads_st, read_lb = [], [], [], [], []
+    ch_score, ch_strand, ch_span, ch_primary, ch_members, ch_count = [], [], [], [], [], []
+    for batch, lb in zip(batches, lookbacks):
+        cfg = ChainingConfig(max_lookback=lb, max_gap=5000)
+        chainer = AffineChainer(cfg, backend="torch", workers=1)
+        for r in range(len(batch)):
+            rp, fp, ln, st = batch.read(r)
+            anchors = AnchorSet.from_lists(rp.astype(np.int64), fp.astype(np.int64),
+                                           ln.astype(np.int64), st.astype(np.int8))
+            chains = chainer.chain(anchors, device="cpu")
+            reads_rp.append(rp)
+            reads_fp.append(fp)
+            reads_ln.append(ln)
+            reads_st.append(st)
+            read_lb.append(lb)
+            ch_count.append(len(chains))
+            for c in chains:
+                ch_score.append(c.score)
+                ch_strand.append(c.strand)
+                ch_span.append([c.read_start, c.read_end, c.ref_start, c.ref_end])
+                ch_primary.append(c.is_primary)
+                ch_members.append(np.asarray(c.anchor_idx, np.int64))
+    rp_flat, read_off = ragged(reads_rp, np.int64)
+    fp_flat, _ = ragged(reads_fp, np.int64)
+    ln_flat, _ = ragged(reads_ln, np.int64)
+    st_flat, _ = ragged(reads_st, np.int8)
+    mem_flat, mem_off = ragged(ch_members, np.int64)
+    np.savez_compressed(
+        os.path.join(HERE, "chain_golden.npz"),
+        lut_default=lut_for(ChainingConfig()),
+        dp_read_end=re_flat, dp_ref_end=fe_flat, dp_weight=w_flat, dp_off=dp_off,
+        dp_has_bonus=has_bonus, dp_bonus=bonus_flat, dp_bonus_off=bonus_off,
+        dp_lookback=np.array([c[4] for c in dp_cases], np.int32),
+        dp_max_gap=np.array([c[5] for c in dp_cases], np.int64),
+        dp_f=f_flat, dp_parent=p_flat,
+        read_pos=rp_flat, ref_pos=fp_flat, length=ln_flat, strand=st_flat, read_off=read_off,
+        read_lookback=np.array(read_lb, np.int32),
+        n_chains=np.array(ch_count, np.int32), chain_score=np.array(ch_score, np.float64),
+        chain_strand=np.array(ch_strand, np.int32), chain_span=np.array(ch_span, np.int64).reshape(-1, 4),
+        chain_primary=np.array(ch_primary, bool), chain_members=mem_flat, chain_members_off=mem_off,
+    )
+    print(f"chain_golden.npz: {len(dp_cases)} DP cases, {len(reads_rp)} reads, {len(ch_score)} chains")
+
+
+# --------------------------------------------------------------------------- #
+# extend_chains (stage level)
+# --------------------------------------------------------------------------- #
+def make_extend(rng):
+    ref = synth.random_reference(300_000, rng)
+    ref_str = synth.decode_bases(ref)
+    cfg = ExtensionConfig()
+    eng = ExtensionEngine(cfg, device="cpu", backend="torch")
+    reads, chain_rows, results = [], [], []
+    for k in range(30):
+        L = int(rng.integers(120, 900))
+        s = int(rng.integers(200, len(ref) - L - 200))
+        prof = (synth.ILLUMINA, synth.HIFI, synth.ONT)[k % 3]
+        tmpl = ref[s: s + L]
+        strand = 1 if k % 2 == 0 else -1
+        if strand < 0:
+            tmpl = synth.reverse_complement(tmpl)
+        read = synth.apply_errors(tmpl, prof, rng)
+        oriented = read if strand > 0 else synth.reverse_complement(read)
+        # a chain of 3 anchors along the true diagonal, with a jittered diagonal
+        n = len(oriented)
+        rp = np.array([5, n // 2, max(n - 40, 6)], np.int64)
+        jit = rng.integers(-6, 7, size=3)
+        fp = s + rp + jit
+        ln = np.array([15, 15, 15], np.int64)
+        anchors = AnchorSet.from_lists(rp, fp, ln, np.full(3, strand, np.int8))
+        chain = Chain(anchor_idx=np.arange(3), score=40.0, strand=strand,
+                      read_start=int(rp.min()), read_end=int((rp + ln).max()),
+                      ref_start=int(fp.min()), ref_end=int((fp + ln).max()))
+        res = eng.extend_chains(synth.decode_bases(read), [chain], anchors, ref_str)[0]
+        reads.append(read)
+        chain_rows.append(np.concatenate([rp, fp, ln, [strand]]))
+        results.append(res)
+    r_flat, r_off = ragged(reads, np.int8)
+    cg_flat, cg_off = ragged([cigar_words(x.cigar) for x in results], np.uint32)
+    np.savez_compressed(
+        os.path.join(HERE, "extend_golden.npz"),
+        ref=ref, reads=r_flat, read_off=r_off, chains=np.array(chain_rows, np.int64),
+        score=np.array([x.score for x in results], np.float64),
+        read_start=np.array([x.read_start for x in results], np.int64),
+        read_end=np.array([x.read_end for x in results], np.int64),
+        ref_start=np.array([x.ref_start for x in results], np.int64),
+        ref_end=np.array([x.ref_end for x in results], np.int64),
+        counts=np.array([[x.n_match, x.n_mismatch, x.n_insertion, x.n_deletion] for x in results]),
+        cigar=cg_flat, cigar_off=cg_off,
+        cfg=np.array([cfg.match_score, cfg.mismatch_penalty, cfg.gap_open, cfg.gap_extend,
+                      cfg.x_drop, cfg.half_band, cfg.max_half_band, cfg.flank, cfg.max_window]),
+    )
+    print(f"extend_golden.npz: {len(results)} single-chain extensions")
+
+
+if __name__ == "__main__":
+    which = sys.argv[1:] or ["sw", "chain", "extend"]
+    if "sw" in which:
+        make_sw(np.random.default_rng(101))
+    if "chain" in which:
+        make_chain(np.random.default_rng(202))
+    if "extend" in which:
+        make_extend(np.random.default_rng(303))
