@@ -1,0 +1,736 @@
+// Anchor chaining for sm_100a: strand split + sort, float64 chaining DP,
+// chain peeling and primary/secondary selection.
+//
+// Semantics (GraphMambaFormer):
+//   sort      alignment/types.py L144-152   for_strand (+1 then -1) and
+//             sorted_by_ref = stable lexsort by (ref_end, read_end)
+//   DP        alignment/chaining.py L129-180 chain_dp_numpy: float64
+//             ((f[j] + min(min(dq,dr), w_i)) - pen[|dr-dq|]) [+ bonus],
+//             argmax = first maximum (lowest j), taken only if > w_i
+//   peel      chaining.py L530-576 _backtrack: argsort(-f, stable), claimed
+//             mask, partial score f[i] - f[stop]
+//   select    chaining.py L579-617 select + _read_overlap
+// The log2 penalty comes from a host table, so the device performs only IEEE
+// float64 add / subtract / compare in the reference's order and the results
+// are bit-identical.
+//
+// Layout: one CTA per read for sort and peel/select (shared-memory bitonic
+// sort of 64-bit keys + 32-bit tie index; reads too large for shared memory
+// sort in their own workspace range), one warp per (read, strand) segment for
+// the DP with the predecessor window in a shared-memory ring.
+
+#include <float.h>
+
+#include <algorithm>
+
+#include "gmf_common.cuh"
+
+namespace gmf {
+
+// ---------------------------------------------------------------------------
+// Block-wide bitonic sort of (key, idx) pairs, ascending, ties by idx.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool pair_less(unsigned long long ka, int ia, unsigned long long kb,
+                                          int ib) {
+    return ka < kb || (ka == kb && ia < ib);
+}
+
+__device__ void block_bitonic(unsigned long long* key, int* idx, int npow2) {
+    for (int k = 2; k <= npow2; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int x = threadIdx.x; x < npow2; x += blockDim.x) {
+                const int y = x ^ j;
+                if (y > x) {
+                    const bool up = (x & k) == 0;
+                    const unsigned long long kx = key[x], ky = key[y];
+                    const int ix = idx[x], iy = idx[y];
+                    const bool swap = up ? pair_less(ky, iy, kx, ix) : pair_less(kx, ix, ky, iy);
+                    if (swap) {
+                        key[x] = ky;
+                        key[y] = kx;
+                        idx[x] = iy;
+                        idx[y] = ix;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+__host__ __device__ inline int next_pow2(int n) {
+    int p = 1;
+    while (p < n) p <<= 1;
+    return p;
+}
+
+// Order-preserving map of a double onto uint64 (ascending), -0.0 == +0.0.
+__device__ __forceinline__ unsigned long long ordered_bits(double v) {
+    if (v == 0.0) v = 0.0;
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+// ---------------------------------------------------------------------------
+// Sort: per read, strand +1 anchors then strand -1 anchors, each by
+// (ref_end, read_end, original index).
+// ---------------------------------------------------------------------------
+struct SortArgs {
+    int32_t n_reads;
+    const int64_t* read_off;
+    const int32_t* read_pos;
+    const int32_t* ref_pos;
+    const int32_t* length;
+    const int8_t* strand;
+    int32_t* perm;
+    int32_t* n_plus;
+    int32_t* n_minus;
+    int32_t* read_end_s;
+    int32_t* ref_end_s;
+    unsigned long long* gkey;  // workspace: 2 * n_anchors keys (large reads)
+    int* gidx;                 // workspace: 2 * n_anchors indices
+    int smem_elems;
+    int* err;
+};
+
+__global__ void __launch_bounds__(256) chain_sort_kernel(SortArgs a) {
+    extern __shared__ unsigned long long sm_keys[];
+    const int r = blockIdx.x;
+    if (r >= a.n_reads) return;
+    const int64_t a0 = a.read_off[r];
+    const int n = (int)(a.read_off[r + 1] - a0);
+    __shared__ int cnt[2];
+    if (threadIdx.x < 2) cnt[threadIdx.x] = 0;
+    if (n > GMF_MAX_READ_ANCHORS) {
+        if (threadIdx.x == 0) {
+            a.n_plus[r] = 0;
+            a.n_minus[r] = 0;
+            if (a.err) atomicOr(a.err, 1);
+        }
+        return;
+    }
+    const int np2 = next_pow2(n > 0 ? n : 1);
+    unsigned long long* key;
+    int* idx;
+    if (np2 <= a.smem_elems) {
+        key = sm_keys;
+        idx = reinterpret_cast<int*>(sm_keys + a.smem_elems);
+    } else if (a.gkey && a.gidx) {
+        key = a.gkey + 2 * a0;
+        idx = a.gidx + 2 * a0;
+    } else {
+        if (threadIdx.x == 0) {
+            a.n_plus[r] = 0;
+            a.n_minus[r] = 0;
+            if (a.err) atomicOr(a.err, 2);
+        }
+        return;
+    }
+    __syncthreads();
+    for (int x = threadIdx.x; x < np2; x += blockDim.x) {
+        unsigned long long k = ~0ull;
+        int ix = 0x7fffffff;
+        if (x < n) {
+            const int8_t s = a.strand[a0 + x];
+            const unsigned long long grp = s == 1 ? 0ull : (s == -1 ? 1ull : 2ull);
+            const unsigned re = (unsigned)(a.read_pos[a0 + x] + a.length[a0 + x]);
+            const unsigned fe = (unsigned)(a.ref_pos[a0 + x] + a.length[a0 + x]);
+            k = (grp << 62) | ((unsigned long long)(fe & 0x7fffffffu) << 31) |
+                (unsigned long long)(re & 0x7fffffffu);
+            ix = x;
+            if (grp < 2) atomicAdd(&cnt[grp], 1);
+        }
+        key[x] = k;
+        idx[x] = ix;
+    }
+    __syncthreads();
+    block_bitonic(key, idx, np2);
+    const int m = cnt[0] + cnt[1];
+    for (int x = threadIdx.x; x < m; x += blockDim.x) {
+        const unsigned long long k = key[x];
+        a.perm[a0 + x] = idx[x];
+        a.ref_end_s[a0 + x] = (int32_t)((k >> 31) & 0x7fffffffu);
+        a.read_end_s[a0 + x] = (int32_t)(k & 0x7fffffffu);
+    }
+    if (threadIdx.x == 0) {
+        a.n_plus[r] = cnt[0];
+        a.n_minus[r] = cnt[1];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Chaining DP: one warp per segment of sorted anchors.
+// ---------------------------------------------------------------------------
+struct DpArgs {
+    // segment source: either explicit rows (row_off) or sorted reads
+    int32_t n_segments;
+    const int64_t* row_off;   // rows mode
+    const int64_t* read_off;  // reads mode
+    const int32_t* n_plus;
+    const int32_t* n_minus;
+    const int32_t* read_end;
+    const int32_t* ref_end;
+    const double* weight;    // NULL: anchor length (reads mode), via length_s
+    const int32_t* length;   // original lengths (reads mode, weight == NULL)
+    const int32_t* perm;     // reads mode
+    const double* bonus;
+    int32_t lookback;
+    int32_t max_gap;
+    const double* lut;
+    int32_t lut_len;
+    double* f;
+    int32_t* parent;
+    int32_t ring;            // ring entries per warp (power of two > lookback)
+};
+
+__device__ __forceinline__ void seg_range(const DpArgs& a, int s, int64_t& start, int& n) {
+    if (a.row_off) {
+        start = a.row_off[s];
+        n = (int)(a.row_off[s + 1] - start);
+    } else {
+        const int r = s >> 1;
+        const int64_t a0 = a.read_off[r];
+        if ((s & 1) == 0) {
+            start = a0;
+            n = a.n_plus[r];
+        } else {
+            start = a0 + a.n_plus[r];
+            n = a.n_minus[r];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128) chain_dp_kernel(DpArgs a) {
+    extern __shared__ double dp_smem[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int wpb = blockDim.x >> 5;
+    const int R = a.ring;
+    const int mask = R - 1;
+    double* rf = dp_smem + (size_t)wib * R * 2;  // f ring, then (read_end, ref_end) as int2
+    int2* rc = reinterpret_cast<int2*>(rf + R);
+    const int lb = a.lookback > 1 ? a.lookback : 1;
+    for (int s = blockIdx.x * wpb + wib; s < a.n_segments; s += gridDim.x * wpb) {
+        int64_t st;
+        int n;
+        seg_range(a, s, st, n);
+        int64_t r0 = 0;
+        if (!a.row_off) r0 = a.read_off[s >> 1];
+        for (int i = 0; i < n; ++i) {
+            const int64_t gi = st + i;
+            const int qi = a.read_end[gi];
+            const int ri = a.ref_end[gi];
+            double wi;
+            if (a.weight)
+                wi = a.weight[gi];
+            else
+                wi = (double)a.length[r0 + a.perm[gi]];
+            const int lo = i - lb > 0 ? i - lb : 0;
+            double best = -DBL_MAX;
+            int bj = -1;
+            bool any = false;
+            for (int j = lo + lane; j < i; j += 32) {
+                const int2 c = rc[j & mask];
+                const int dq = qi - c.x;
+                const int dr = ri - c.y;
+                double sc;
+                if (dq > 0 && dr > 0 && dq <= a.max_gap && dr <= a.max_gap) {
+                    any = true;
+                    const double mn = (double)(dq < dr ? dq : dr);
+                    const double adv = mn < wi ? mn : wi;
+                    const int gap = dr > dq ? dr - dq : dq - dr;
+                    sc = __dsub_rn(__dadd_rn(rf[j & mask], adv), __ldg(&a.lut[gap]));
+                    if (a.bonus) sc = __dadd_rn(sc, __ldg(&a.bonus[gi * lb + (lb - (i - lo)) + (j - lo)]));
+                } else {
+                    sc = -1e30;
+                }
+                if (bj < 0 || sc > best) {
+                    best = sc;
+                    bj = j;
+                }
+            }
+            any = __any_sync(FULL_MASK, any);
+            double fi = wi;
+            int pi = -1;
+            if (any) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const double ob = __shfl_xor_sync(FULL_MASK, best, o);
+                    const int oj = __shfl_xor_sync(FULL_MASK, bj, o);
+                    const bool take = (oj >= 0) && (bj < 0 || ob > best || (ob == best && oj < bj));
+                    if (take) {
+                        best = ob;
+                        bj = oj;
+                    }
+                }
+                if (best > wi) {
+                    fi = best;
+                    pi = bj;
+                }
+            }
+            if (lane == 0) {
+                rf[i & mask] = fi;
+                rc[i & mask] = make_int2(qi, ri);
+                a.f[gi] = fi;
+                a.parent[gi] = pi;
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Chain peeling + select: one CTA per read.
+// ---------------------------------------------------------------------------
+struct PeelArgs {
+    int32_t n_reads;
+    const int64_t* read_off;
+    const int32_t* n_plus;
+    const int32_t* n_minus;
+    const int32_t* perm;
+    const int32_t* read_pos;  // original layout
+    const int32_t* ref_pos;
+    const int32_t* length;
+    const double* f;
+    const int32_t* parent;
+    int32_t min_chain_anchors;
+    int32_t max_chains;
+    double min_chain_score;
+    double secondary_overlap;
+    double secondary_score_ratio;
+    // workspace (per anchor, in the read's range)
+    unsigned long long* gkey;  // 2 * n_anchors
+    int* gidx;                 // 2 * n_anchors
+    int32_t* mem_tmp;          // candidate members (sorted-local indices)
+    double* c_score;           // candidate records
+    int4* c_span;
+    int2* c_mem;               // (member offset within read, count)
+    int8_t* c_strand;
+    int8_t* claimed;           // per anchor
+    int smem_elems;
+    // results
+    int32_t* n_chains;
+    double* score;
+    int32_t* strand;
+    int32_t* span;
+    int32_t* is_primary;
+    int32_t* n_members;
+    int32_t* members;
+};
+
+__global__ void __launch_bounds__(256) chain_peel_kernel(PeelArgs a) {
+    extern __shared__ unsigned long long pk_smem[];
+    const int r = blockIdx.x;
+    if (r >= a.n_reads) return;
+    const int64_t a0 = a.read_off[r];
+    __shared__ int n_cand;
+    __shared__ int n_memtot;
+    if (threadIdx.x == 0) {
+        n_cand = 0;
+        n_memtot = 0;
+    }
+    const int np = a.n_plus[r], nm = a.n_minus[r];
+    const int n_sorted = np + nm;
+    // claimed flags reuse the tie-index array after the sort (one byte each)
+    for (int seg = 0; seg < 2; ++seg) {
+        const int n = seg == 0 ? np : nm;
+        const int s0 = seg == 0 ? 0 : np;  // offset of the segment inside the read
+        __syncthreads();
+        if (n < a.min_chain_anchors || n == 0) continue;
+        const int np2 = next_pow2(n);
+        unsigned long long* key;
+        int* idx;
+        if (np2 <= a.smem_elems) {
+            key = pk_smem;
+            idx = reinterpret_cast<int*>(pk_smem + a.smem_elems);
+        } else {
+            key = a.gkey + 2 * a0;
+            idx = a.gidx + 2 * a0;
+        }
+        for (int x = threadIdx.x; x < np2; x += blockDim.x) {
+            if (x < n) {
+                // argsort(-f, stable): ascending -f == descending f, ties by index
+                key[x] = ~ordered_bits(a.f[a0 + s0 + x]);
+                idx[x] = x;
+            } else {
+                key[x] = ~0ull;
+                idx[x] = 0x7fffffff;
+            }
+        }
+        __syncthreads();
+        block_bitonic(key, idx, np2);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int8_t* claimed = a.claimed + a0;
+            for (int x = 0; x < n; ++x) claimed[x] = 0;
+            const double* f = a.f + a0 + s0;
+            const int32_t* par = a.parent + a0 + s0;
+            for (int k = 0; k < n; ++k) {
+                const int i = idx[k];
+                if (claimed[i]) continue;
+                int m = 0;
+                int node = i;
+                const int moff = n_memtot;
+                while (node >= 0 && !claimed[node]) {
+                    claimed[node] = 1;
+                    a.mem_tmp[a0 + moff + m] = node;
+                    ++m;
+                    node = par[node];
+                }
+                const double sc = f[i] - (node >= 0 ? f[node] : 0.0);
+                if (m < a.min_chain_anchors || sc < a.min_chain_score) continue;
+                // spans over the members (original coordinates)
+                int rs = 0x7fffffff, re = -0x7fffffff - 1, fs = 0x7fffffff, fe = -0x7fffffff - 1;
+                for (int x = 0; x < m; ++x) {
+                    const int o = a.perm[a0 + s0 + a.mem_tmp[a0 + moff + x]];
+                    const int rp = a.read_pos[a0 + o], fp = a.ref_pos[a0 + o], ln = a.length[a0 + o];
+                    rs = min(rs, rp);
+                    re = max(re, rp + ln);
+                    fs = min(fs, fp);
+                    fe = max(fe, fp + ln);
+                }
+                const int c = n_cand++;
+                a.c_score[a0 + c] = sc;
+                a.c_span[a0 + c] = make_int4(rs, re, fs, fe);
+                a.c_mem[a0 + c] = make_int2(moff, m);
+                a.c_strand[a0 + c] = (int8_t)(seg == 0 ? 1 : -1);
+                n_memtot += m;
+            }
+        }
+        __syncthreads();
+    }
+    __syncthreads();
+    // ---- select ----
+    const int nc = n_cand;
+    if (nc == 0) {
+        if (threadIdx.x == 0) a.n_chains[r] = 0;
+        return;
+    }
+    const int np2 = next_pow2(nc);
+    unsigned long long* key;
+    int* idx;
+    if (np2 <= a.smem_elems) {
+        key = pk_smem;
+        idx = reinterpret_cast<int*>(pk_smem + a.smem_elems);
+    } else {
+        key = a.gkey + 2 * a0;
+        idx = a.gidx + 2 * a0;
+    }
+    for (int x = threadIdx.x; x < np2; x += blockDim.x) {
+        if (x < nc) {
+            key[x] = ~ordered_bits(a.c_score[a0 + x]);  // sorted(key=-score), stable
+            idx[x] = x;
+        } else {
+            key[x] = ~0ull;
+            idx[x] = 0x7fffffff;
+        }
+    }
+    __syncthreads();
+    block_bitonic(key, idx, np2);
+    __shared__ int kept_c[64];
+    __shared__ int n_kept;
+    if (threadIdx.x == 0) {
+        const int mc = a.max_chains < 64 ? a.max_chains : 64;
+        int kept = 0;
+        const double cutoff = a.c_score[a0 + idx[0]] * a.secondary_score_ratio;
+        for (int k = 0; k < nc; ++k) {
+            const int c = idx[k];
+            const double sc = a.c_score[a0 + c];
+            if (sc < cutoff && kept) break;
+            double overlap = 0.0;
+            if (kept) {  // only the first kept chain is primary
+                const int4 x = a.c_span[a0 + c];
+                const int4 y = a.c_span[a0 + kept_c[0]];
+                const int lo = max(x.x, y.x), hi = min(x.y, y.y);
+                if (hi > lo) {
+                    const int den = max(min(x.y - x.x, y.y - y.x), 1);
+                    overlap = (double)(hi - lo) / (double)den;
+                }
+            }
+            if (overlap > a.secondary_overlap) continue;
+            kept_c[kept++] = c;
+            if (kept >= mc) break;
+        }
+        n_kept = kept;
+        a.n_chains[r] = kept;
+    }
+    __syncthreads();
+    // ---- output: records and members (original indices, read order) ----
+    int wpos = 0;
+    for (int k = 0; k < n_kept; ++k) {
+        const int c = kept_c[k];
+        const int2 cm = a.c_mem[a0 + c];
+        const int s0 = a.c_strand[a0 + c] == 1 ? 0 : np;
+        const size_t slot = (size_t)r * a.max_chains + k;
+        if (threadIdx.x == 0) {
+            a.score[slot] = a.c_score[a0 + c];
+            a.strand[slot] = a.c_strand[a0 + c];
+            const int4 sp = a.c_span[a0 + c];
+            a.span[4 * slot + 0] = sp.x;
+            a.span[4 * slot + 1] = sp.y;
+            a.span[4 * slot + 2] = sp.z;
+            a.span[4 * slot + 3] = sp.w;
+            a.is_primary[slot] = k == 0;
+            a.n_members[slot] = cm.y;
+        }
+        // the walk stored members from chain end to start: reverse to read order
+        for (int x = threadIdx.x; x < cm.y; x += blockDim.x) {
+            const int loc = a.mem_tmp[a0 + cm.x + (cm.y - 1 - x)];
+            a.members[a0 + wpos + x] = a.perm[a0 + s0 + loc];
+        }
+        wpos += cm.y;
+    }
+    (void)n_sorted;
+}
+
+}  // namespace gmf
+
+using namespace gmf;
+
+namespace {
+
+int sort_smem_elems() { return 8192; }  // 8192 * 12 B = 96 KB
+
+size_t sort_smem_bytes(int elems) { return (size_t)elems * (sizeof(unsigned long long) + sizeof(int)); }
+
+int launch_sort(const gmf_anchor_batch* an, const gmf_sorted_anchors* so, unsigned long long* gkey,
+                int* gidx, int* err, cudaStream_t stream) {
+    SortArgs s;
+    s.n_reads = an->n_reads;
+    s.read_off = an->read_off;
+    s.read_pos = an->read_pos;
+    s.ref_pos = an->ref_pos;
+    s.length = an->length;
+    s.strand = an->strand;
+    s.perm = so->perm;
+    s.n_plus = so->n_plus;
+    s.n_minus = so->n_minus;
+    s.read_end_s = so->read_end;
+    s.ref_end_s = so->ref_end;
+    s.gkey = gkey;
+    s.gidx = gidx;
+    s.smem_elems = sort_smem_elems();
+    s.err = err;
+    const size_t smem = sort_smem_bytes(s.smem_elems);
+    GMF_CUDA_TRY(cudaFuncSetAttribute(chain_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+    chain_sort_kernel<<<an->n_reads, 256, smem, stream>>>(s);
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_dp(DpArgs d, int n_segments, cudaStream_t stream) {
+    d.n_segments = n_segments;
+    int lb = d.lookback > 1 ? d.lookback : 1;
+    d.ring = next_pow2(lb + 1);
+    const int wpb = 4;
+    const size_t smem = (size_t)wpb * d.ring * (sizeof(double) + sizeof(int2));
+    GMF_CUDA_TRY(cudaFuncSetAttribute(chain_dp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+    const int blocks = (n_segments + wpb - 1) / wpb;
+    if (blocks > 0) chain_dp_kernel<<<blocks, 32 * wpb, smem, stream>>>(d);
+    return cuda_status(cudaGetLastError());
+}
+
+bool valid_lut(const double* lut, int32_t lut_len, int32_t max_gap) {
+    return lut != nullptr && lut_len >= max_gap + 1;
+}
+
+size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+}  // namespace
+
+extern "C" int gmf_chain_dp(int32_t n_rows, const int64_t* row_off, const int32_t* read_end,
+                            const int32_t* ref_end, const double* weight, const double* bonus,
+                            int32_t max_lookback, int32_t max_gap, const double* pen_lut,
+                            int32_t lut_len, double* f, int32_t* parent, gmf_stream_t stream) {
+    if (n_rows < 0 || max_gap < 0) return GMF_ERR_INVALID_ARGUMENT;
+    if (max_lookback > GMF_MAX_LOOKBACK) return GMF_ERR_LIMIT;
+    if (n_rows == 0) return GMF_OK;
+    if (!row_off || !read_end || !ref_end || !weight || !f || !parent) return GMF_ERR_INVALID_ARGUMENT;
+    if (!valid_lut(pen_lut, lut_len, max_gap)) return GMF_ERR_INVALID_ARGUMENT;
+    GMF_TRY(bind_stream_device((cudaStream_t)stream));
+    DpArgs d{};
+    d.row_off = row_off;
+    d.read_end = read_end;
+    d.ref_end = ref_end;
+    d.weight = weight;
+    d.bonus = bonus;
+    d.lookback = max_lookback;
+    d.max_gap = max_gap;
+    d.lut = pen_lut;
+    d.lut_len = lut_len;
+    d.f = f;
+    d.parent = parent;
+    return launch_dp(d, n_rows, (cudaStream_t)stream);
+}
+
+extern "C" int gmf_chain_sort(const gmf_anchor_batch* an, const gmf_sorted_anchors* so,
+                              void* workspace, size_t workspace_bytes, gmf_stream_t stream) {
+    if (!an || !so || an->n_reads < 0) return GMF_ERR_INVALID_ARGUMENT;
+    if (an->n_reads == 0) return GMF_OK;
+    if (!an->read_off || !an->read_pos || !an->ref_pos || !an->length || !an->strand ||
+        !so->perm || !so->n_plus || !so->n_minus || !so->read_end || !so->ref_end)
+        return GMF_ERR_INVALID_ARGUMENT;
+    if (!workspace || workspace_bytes < 256) return GMF_ERR_WORKSPACE;
+    GMF_TRY(bind_stream_device((cudaStream_t)stream));
+    // reads too large for shared memory sort in 12 * 2 bytes per anchor of
+    // workspace (gmf_chain_workspace_bytes covers it)
+    const size_t A = (workspace_bytes - 256) / 24;
+    char* p = (char*)workspace;
+    int* err = (int*)p;
+    unsigned long long* gkey = (unsigned long long*)(p + 256);
+    int* gidx = (int*)(p + 256 + align256(2 * A * 8));
+    if (256 + align256(2 * A * 8) + 2 * A * 4 > workspace_bytes) {
+        gidx = nullptr;
+        gkey = nullptr;
+    }
+    GMF_CUDA_TRY(cudaMemsetAsync(err, 0, 4, (cudaStream_t)stream));
+    return launch_sort(an, so, gkey, gidx, err, (cudaStream_t)stream);
+}
+
+extern "C" size_t gmf_chain_workspace_bytes(int32_t n_reads, int64_t n_anchors) {
+    const size_t A = (size_t)(n_anchors > 0 ? n_anchors : 0);
+    const size_t R = (size_t)(n_reads > 0 ? n_reads : 0);
+    size_t b = 256;                       // error word
+    b += align256(2 * A * 8);             // gkey
+    b += align256(2 * A * 4);             // gidx
+    b += align256(A * 4) * 3;             // perm, read_end_s, ref_end_s
+    b += align256(R * 4) * 2;             // n_plus, n_minus
+    b += align256(A * 8);                 // f
+    b += align256(A * 4);                 // parent
+    b += align256(A * 4);                 // mem_tmp
+    b += align256(A * 8);                 // c_score
+    b += align256(A * 16);                // c_span
+    b += align256(A * 8);                 // c_mem
+    b += align256(2 * A);                 // c_strand + claimed flags
+    return b;
+}
+
+extern "C" int gmf_chain_batch(const gmf_anchor_batch* an, const gmf_chain_params* cp,
+                               const double* pen_lut, int32_t lut_len,
+                               const gmf_sorted_anchors* sorted_in, const double* sorted_weight,
+                               const double* sorted_bonus, const gmf_chain_results* res,
+                               void* workspace, size_t workspace_bytes, gmf_stream_t stream_) {
+    const cudaStream_t stream = (cudaStream_t)stream_;
+    if (!an || !cp || !res || an->n_reads < 0) return GMF_ERR_INVALID_ARGUMENT;
+    if (cp->max_lookback > GMF_MAX_LOOKBACK) return GMF_ERR_LIMIT;
+    if (cp->max_gap < 0 || cp->max_chains < 1 || cp->max_chains > 64) return GMF_ERR_INVALID_ARGUMENT;
+    if (an->n_reads == 0) return GMF_OK;
+    if (!an->read_off || !an->read_pos || !an->ref_pos || !an->length || !an->strand)
+        return GMF_ERR_INVALID_ARGUMENT;
+    if (!res->n_chains || !res->score || !res->strand || !res->span || !res->is_primary ||
+        !res->n_members || !res->members)
+        return GMF_ERR_INVALID_ARGUMENT;
+    if (!valid_lut(pen_lut, lut_len, cp->max_gap)) return GMF_ERR_INVALID_ARGUMENT;
+    if ((sorted_weight || sorted_bonus) && !sorted_in) return GMF_ERR_INVALID_ARGUMENT;
+    if (!workspace) return GMF_ERR_WORKSPACE;
+    GMF_TRY(bind_stream_device(stream));
+
+    // the host does not know n_anchors (device CSR); the caller sized the
+    // workspace with gmf_chain_workspace_bytes, so derive A from its size.
+    // Layout is computed for the largest A that fits.
+    const size_t R = (size_t)an->n_reads;
+    size_t lo = 0, hi = workspace_bytes;
+    while (lo < hi) {  // largest A with bytes(R, A) <= workspace_bytes
+        const size_t mid = (lo + hi + 1) / 2;
+        if (gmf_chain_workspace_bytes((int32_t)R, (int64_t)mid) <= workspace_bytes)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const size_t A = lo;
+    char* p = (char*)workspace;
+    int* err = (int*)p;
+    p += 256;
+    auto take = [&](size_t bytes) {
+        char* q = p;
+        p += align256(bytes);
+        return q;
+    };
+    unsigned long long* gkey = (unsigned long long*)take(2 * A * 8);
+    int* gidx = (int*)take(2 * A * 4);
+    gmf_sorted_anchors so;
+    int32_t* perm_w = (int32_t*)take(A * 4);
+    int32_t* re_w = (int32_t*)take(A * 4);
+    int32_t* fe_w = (int32_t*)take(A * 4);
+    int32_t* npl_w = (int32_t*)take(R * 4);
+    int32_t* nmi_w = (int32_t*)take(R * 4);
+    double* f = (double*)take(A * 8);
+    int32_t* parent = (int32_t*)take(A * 4);
+    int32_t* mem_tmp = (int32_t*)take(A * 4);
+    double* c_score = (double*)take(A * 8);
+    int4* c_span = (int4*)take(A * 16);
+    int2* c_mem = (int2*)take(A * 8);
+    int8_t* c_strand = (int8_t*)take(2 * A);
+    if (sorted_in) {
+        so = *sorted_in;
+    } else {
+        so.perm = perm_w;
+        so.n_plus = npl_w;
+        so.n_minus = nmi_w;
+        so.read_end = re_w;
+        so.ref_end = fe_w;
+    }
+    GMF_CUDA_TRY(cudaMemsetAsync(err, 0, 256, stream));
+    int st;
+    if (!sorted_in) {
+        st = launch_sort(an, &so, gkey, gidx, err, stream);
+        if (st) return st;
+    }
+    DpArgs d{};
+    d.read_off = an->read_off;
+    d.n_plus = so.n_plus;
+    d.n_minus = so.n_minus;
+    d.read_end = so.read_end;
+    d.ref_end = so.ref_end;
+    d.weight = sorted_weight;
+    d.length = an->length;
+    d.perm = so.perm;
+    d.bonus = sorted_bonus;
+    d.lookback = cp->max_lookback;
+    d.max_gap = cp->max_gap;
+    d.lut = pen_lut;
+    d.lut_len = lut_len;
+    d.f = f;
+    d.parent = parent;
+    st = launch_dp(d, 2 * an->n_reads, stream);
+    if (st) return st;
+
+    PeelArgs k{};
+    k.n_reads = an->n_reads;
+    k.read_off = an->read_off;
+    k.n_plus = so.n_plus;
+    k.n_minus = so.n_minus;
+    k.perm = so.perm;
+    k.read_pos = an->read_pos;
+    k.ref_pos = an->ref_pos;
+    k.length = an->length;
+    k.f = f;
+    k.parent = parent;
+    k.min_chain_anchors = cp->min_chain_anchors;
+    k.max_chains = cp->max_chains;
+    k.min_chain_score = cp->min_chain_score;
+    k.secondary_overlap = cp->secondary_overlap;
+    k.secondary_score_ratio = cp->secondary_score_ratio;
+    k.gkey = gkey;
+    k.gidx = gidx;
+    k.mem_tmp = mem_tmp;
+    k.c_score = c_score;
+    k.c_span = c_span;
+    k.c_mem = c_mem;
+    k.c_strand = c_strand;
+    k.claimed = c_strand + A;
+    k.smem_elems = sort_smem_elems();
+    k.n_chains = res->n_chains;
+    k.score = res->score;
+    k.strand = res->strand;
+    k.span = res->span;
+    k.is_primary = res->is_primary;
+    k.n_members = res->n_members;
+    k.members = res->members;
+    const size_t smem = sort_smem_bytes(k.smem_elems);
+    GMF_CUDA_TRY(cudaFuncSetAttribute(chain_peel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+    chain_peel_kernel<<<an->n_reads, 256, smem, stream>>>(k);
+    return cuda_status(cudaGetLastError());
+}

@@ -1,0 +1,222 @@
+"""Throughput API: reusable sessions for repeated batches.
+
+A session keeps pinned host staging buffers, device input/output buffers and
+the workspace alive between calls (all grow-only), so a steady stream of
+batches pays only the copies and the kernels.  ``align`` / ``chain`` take
+host arrays and return host arrays: this is the end-to-end path a service
+calls, and the one ``bench.py`` measures as ``e2e``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _native
+from .chaining import AnchorCSR, ChainResult, ChainingConfig, LUTS, chain_params
+from .device import bind, require_cuda
+from .extension import SWResult, longest_first, sw_params
+from .synth import PairSet
+
+
+class _Buffers:
+    """Grow-only pinned host + device buffer pairs, one per named slot."""
+
+    def __init__(self, device: torch.device):
+        self.device = device
+        self.host: dict[str, torch.Tensor] = {}
+        self.dev: dict[str, torch.Tensor] = {}
+
+    def _grow(self, table, name, n, dtype, pinned):
+        t = table.get(name)
+        if t is None or t.numel() < n or t.dtype != dtype:
+            size = max(n, int(t.numel() * 1.25) if t is not None and t.dtype == dtype else n, 1)
+            if pinned:
+                t = torch.empty(size, dtype=dtype, pin_memory=True)
+            else:
+                t = torch.empty(size, dtype=dtype, device=self.device)
+            table[name] = t
+        return t
+
+    def upload(self, name: str, a: np.ndarray, stream) -> torch.Tensor:
+        """Stage ``a`` in pinned memory and copy it to the device buffer."""
+        a = np.ascontiguousarray(a)
+        dt = torch.from_numpy(a[:0]).dtype if a.size == 0 else torch.from_numpy(a).dtype
+        n = a.size
+        h = self._grow(self.host, name, n, dt, True)
+        d = self._grow(self.dev, name, n, dt, False)
+        if n:
+            h[:n].numpy()[...] = a.reshape(-1)
+            with torch.cuda.stream(stream):
+                d[:n].copy_(h[:n], non_blocking=True)
+        return d
+
+    def device_buf(self, name: str, n: int, dtype) -> torch.Tensor:
+        return self._grow(self.dev, name, n, dtype, False)
+
+    def download(self, name: str, d: torch.Tensor, n: int, stream) -> torch.Tensor:
+        h = self._grow(self.host, name, n, d.dtype, True)
+        if n:
+            with torch.cuda.stream(stream):
+                h[:n].copy_(d[:n], non_blocking=True)
+        return h
+
+
+class ExtensionSession:
+    """Repeated banded SW + traceback on host batches."""
+
+    def __init__(self, device=None, match_score=2.0, mismatch_penalty=4.0, gap_open=6.0,
+                 gap_extend=2.0, x_drop=0.0, traceback: bool = True,
+                 stream: Optional[torch.cuda.Stream] = None):
+        self.device = require_cuda(device)
+        self.params = sw_params(match_score, mismatch_penalty, gap_open, gap_extend, x_drop)
+        self.traceback = traceback
+        self.stream = stream or torch.cuda.Stream(self.device)
+        self.buf = _Buffers(self.device)
+        self.h2d_bytes = 0
+        self.d2h_bytes = 0
+
+    def align(self, pairs: PairSet, order: Optional[np.ndarray] = None) -> SWResult:
+        B = len(pairs)
+        s = self.stream
+        qlen = np.diff(pairs.query_off).astype(np.int32)
+        tlen = np.diff(pairs.target_off).astype(np.int32)
+        hb = np.asarray(pairs.half_band, np.int32)
+        if B and (hb.min() < 0 or hb.max() > _native.MAX_HALF_BAND):
+            raise ValueError(f"half_band must be within [0, {_native.MAX_HALF_BAND}]")
+        if order is None and B:
+            order = longest_first(qlen, hb)
+        up = self.buf.upload
+        q = up("q", pairs.query.astype(np.int8, copy=False), s)
+        qo = up("qo", pairs.query_off.astype(np.int64, copy=False), s)
+        t = up("t", pairs.target.astype(np.int8, copy=False), s)
+        to = up("to", pairs.target_off.astype(np.int64, copy=False), s)
+        hbd = up("hb", hb, s)
+        off = up("off", np.asarray(pairs.band_offset, np.int32), s)
+        od = up("order", np.asarray(order if order is not None else np.zeros(0), np.int32), s)
+        self.h2d_bytes = int(pairs.query.size + pairs.target.size + 16 * (B + 1) + 12 * B)
+        n = max(B, 1)
+        cap = int(qlen.astype(np.int64).sum() + tlen.astype(np.int64).sum() + B) if self.traceback else 0
+        db = self.buf.device_buf
+        out = {k: db(k, n, torch.int32) for k in ("score", "qe", "te", "qs", "ts", "clen")}
+        counts = db("counts", 4 * n, torch.int32)
+        cstart = db("cstart", n, torch.int64)
+        cigar = db("cigar", max(cap, 1), torch.int32)
+        used = db("used", 1, torch.int64)
+        err = db("err", 1, torch.int32)
+        need = int(_native.lib().gmf_banded_sw_workspace_bytes(
+            B, qlen.ctypes.data_as(ctypes.c_void_p), tlen.ctypes.data_as(ctypes.c_void_p),
+            hb.ctypes.data_as(ctypes.c_void_p), 1 if self.traceback else 0))
+        ws = db("ws", need, torch.uint8)
+        pairs_c = _native.GmfPairs(B, q.data_ptr(), qo.data_ptr(), t.data_ptr(), to.data_ptr(),
+                                   hbd.data_ptr(), off.data_ptr(), od.data_ptr() if B else None,
+                                   int(hb.max()) if B else 0)
+        tb = self.traceback
+        res_c = _native.GmfSwResults(
+            out["score"].data_ptr(), out["qe"].data_ptr(), out["te"].data_ptr(),
+            out["qs"].data_ptr() if tb else None, out["ts"].data_ptr() if tb else None,
+            counts.data_ptr() if tb else None, cigar.data_ptr() if tb else None,
+            cigar.numel() if tb else 0, cstart.data_ptr() if tb else None,
+            out["clen"].data_ptr() if tb else None, used.data_ptr(), err.data_ptr())
+        sp = int(s.cuda_stream)
+        bind(self.device, sp)
+        st = _native.lib().gmf_banded_sw(ctypes.byref(pairs_c), ctypes.byref(self.params),
+                                         ctypes.byref(res_c), ctypes.c_void_p(ws.data_ptr()),
+                                         ws.numel(), ctypes.c_void_p(sp))
+        _native.check("gmf_banded_sw", st)
+        dl = self.buf.download
+        names = ["score", "qe", "te"] + (["qs", "ts", "clen"] if tb else [])
+        host = {k: dl("h_" + k, out[k], B, s) for k in names}
+        h_used = dl("h_used", used, 1, s)
+        h_err = dl("h_err", err, 1, s)
+        if tb:
+            h_counts = dl("h_counts", counts, 4 * B, s)
+            h_cstart = dl("h_cstart", cstart, B, s)
+        s.synchronize()
+        res = SWResult(host["score"][:B].numpy().copy(), host["qe"][:B].numpy().copy(),
+                       host["te"][:B].numpy().copy(), error_flags=int(h_err[0]))
+        nbytes = 12 * B + 12
+        if tb:
+            nu = int(h_used[0])
+            h_cig = dl("h_cigar", cigar, nu, s)
+            s.synchronize()
+            res.query_start = host["qs"][:B].numpy().copy()
+            res.target_start = host["ts"][:B].numpy().copy()
+            res.cigar_len = host["clen"][:B].numpy().copy()
+            res.op_counts = h_counts[: 4 * B].numpy().reshape(B, 4).copy()
+            res.cigar_start = h_cstart[:B].numpy().copy()
+            res.cigar_words = h_cig[:nu].numpy().view(np.uint32).copy()
+            nbytes += 36 * B + 4 * nu
+        self.d2h_bytes = nbytes
+        res.d2h_bytes = nbytes
+        if res.error_flags:
+            raise RuntimeError(f"gmf_banded_sw reported error flags {res.error_flags}")
+        return res
+
+
+class ChainSession:
+    """Repeated fast-mode chaining (sort, DP, peel, select) on host batches."""
+
+    def __init__(self, cfg: Optional[ChainingConfig] = None, device=None,
+                 stream: Optional[torch.cuda.Stream] = None):
+        self.cfg = cfg or ChainingConfig()
+        self.device = require_cuda(device)
+        self.stream = stream or torch.cuda.Stream(self.device)
+        self.buf = _Buffers(self.device)
+        self.cp = chain_params(self.cfg)
+        self.lut = LUTS.get(self.device, self.cfg.max_gap, self.cfg.gap_open, self.cfg.gap_extend,
+                            self.cfg.log_coeff)
+        self.h2d_bytes = 0
+        self.d2h_bytes = 0
+
+    def chain(self, batch) -> ChainResult:
+        a = AnchorCSR.of(batch)
+        R, A = len(a), int(a.read_off[-1])
+        if R and np.diff(a.read_off).max() > _native.MAX_READ_ANCHORS:
+            raise ValueError(f"a read has more than {_native.MAX_READ_ANCHORS} anchors")
+        s = self.stream
+        up = self.buf.upload
+        ro = up("ro", a.read_off, s)
+        rp = up("rp", a.read_pos, s)
+        fp = up("fp", a.ref_pos, s)
+        ln = up("ln", a.length, s)
+        st = up("st", a.strand, s)
+        self.h2d_bytes = int(a.read_off.nbytes + a.read_pos.nbytes + a.ref_pos.nbytes
+                             + a.length.nbytes + a.strand.nbytes)
+        mc = self.cp.max_chains
+        db = self.buf.device_buf
+        nR, nA = max(R, 1), max(A, 1)
+        o = dict(n=db("n", nR, torch.int32), score=db("score", nR * mc, torch.float64),
+                 strand=db("strand", nR * mc, torch.int32), span=db("span", 4 * nR * mc, torch.int32),
+                 prim=db("prim", nR * mc, torch.int32), nmem=db("nmem", nR * mc, torch.int32),
+                 mem=db("mem", nA, torch.int32))
+        need = int(_native.lib().gmf_chain_workspace_bytes(R, A))
+        ws = db("ws", need, torch.uint8)
+        batch_c = _native.GmfAnchorBatch(R, ro.data_ptr(), rp.data_ptr(), fp.data_ptr(), ln.data_ptr(),
+                                         st.data_ptr())
+        res_c = _native.GmfChainResults(o["n"].data_ptr(), o["score"].data_ptr(), o["strand"].data_ptr(),
+                                        o["span"].data_ptr(), o["prim"].data_ptr(), o["nmem"].data_ptr(),
+                                        o["mem"].data_ptr())
+        sp = int(s.cuda_stream)
+        bind(self.device, sp)
+        rc = _native.lib().gmf_chain_batch(ctypes.byref(batch_c), ctypes.byref(self.cp),
+                                           ctypes.c_void_p(self.lut.data_ptr()), self.lut.numel(), None,
+                                           None, None, ctypes.byref(res_c), ctypes.c_void_p(ws.data_ptr()),
+                                           need, ctypes.c_void_p(sp))
+        _native.check("gmf_chain_batch", rc)
+        dl = self.buf.download
+        sizes = dict(n=R, score=R * mc, strand=R * mc, span=4 * R * mc, prim=R * mc, nmem=R * mc, mem=A)
+        h = {k: dl("h_" + k, o[k], sizes[k], s) for k in sizes}
+        s.synchronize()
+        self.d2h_bytes = int(sum(h[k][: sizes[k]].numel() * h[k].element_size() for k in sizes))
+        return ChainResult(a.read_off, h["n"][:R].numpy().copy(),
+                           h["score"][: R * mc].numpy().reshape(R, mc).copy(),
+                           h["strand"][: R * mc].numpy().reshape(R, mc).copy(),
+                           h["span"][: 4 * R * mc].numpy().reshape(R, mc, 4).copy(),
+                           h["prim"][: R * mc].numpy().reshape(R, mc).copy(),
+                           h["nmem"][: R * mc].numpy().reshape(R, mc).copy(),
+                           h["mem"][:A].numpy().copy(), self.d2h_bytes)

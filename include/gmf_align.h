@@ -1,0 +1,224 @@
+/*
+ * gmf_align.h -- C ABI of the B200 (sm_100a) alignment hot path:
+ * minimap2-style anchor-chaining DP and banded affine-gap Smith-Waterman
+ * extension with CIGAR traceback.
+ *
+ * Conventions
+ *   - Every pointer in a gmf_* struct or argument is a DEVICE pointer unless
+ *     its comment says "host".  Buffers are owned by the caller.
+ *   - Work is enqueued on the caller's stream; no entry point synchronises
+ *     except where documented (none of the compute calls do).
+ *   - Every entry point returns an int status, GMF_OK (0) on success.  No C++
+ *     exception crosses this boundary.  gmf_status_string() names a status.
+ *   - Results are deterministic per pair / per read and independent of the
+ *     other work in the same call (band, x-drop and tie rules are applied per
+ *     pair), so a pair aligned alone or inside a large batch gives the same
+ *     score, coordinates and CIGAR.
+ *   - No call allocates device memory: scratch lives in the caller's
+ *     workspace (size it with the *_workspace_bytes helpers).
+ *
+ * Reference interfaces these entry points replace (GraphMambaFormer):
+ *   gmf_banded_sw     graphmambaformer/accel/cuda_kernels.py L504-566 (banded_sw)
+ *                     + alignment/extension.py L78-302
+ *                     (banded_affine_sw_batch + traceback_banded)
+ *   gmf_chain_dp      accel/cuda_kernels.py L440-501 (chain_dp)
+ *                     + alignment/chaining.py L129-180 (chain_dp_numpy)
+ *   gmf_chain_sort    alignment/types.py L144-152 (for_strand, sorted_by_ref)
+ *   gmf_chain_batch   alignment/chaining.py L620-745 (AffineChainer.chain /
+ *                     chain_batch: sort, DP, _backtrack, select)
+ */
+#ifndef GMF_ALIGN_H
+#define GMF_ALIGN_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* gmf_stream_t; /* a cudaStream_t; NULL = legacy default stream */
+
+/* ---- status codes ------------------------------------------------------ */
+#define GMF_OK 0
+#define GMF_ERR_INVALID_ARGUMENT 1 /* malformed request (NULL pointer, bad size, bad parameter) */
+#define GMF_ERR_CUDA 2             /* a CUDA runtime call failed */
+#define GMF_ERR_WORKSPACE 3        /* workspace smaller than required */
+#define GMF_ERR_CAPACITY 4         /* an output buffer (CIGAR words, chains) is too small */
+#define GMF_ERR_LIMIT 5            /* input beyond a documented size limit */
+#define GMF_ERR_TIMEOUT 6          /* a bounded device-side wait expired */
+#define GMF_ERR_NOT_READY 7        /* asynchronous work still in flight */
+
+const char* gmf_status_string(int status);
+int gmf_version(void); /* major*10000 + minor*100 + patch */
+
+/* The library links its own CUDA runtime.  Calls given a non-NULL stream run
+ * on that stream's device; calls on the legacy stream (NULL) run on the
+ * device selected here (default 0). */
+int gmf_set_device(int device);
+
+/* Limits enforced by the entry points (GMF_ERR_LIMIT beyond them). */
+#define GMF_MAX_HALF_BAND 4096      /* band width W = 2*half_band+1 <= 8193 */
+#define GMF_MAX_SEQ_LEN (1 << 28)   /* query / target length */
+#define GMF_MAX_READ_ANCHORS 16384  /* anchors per read for gmf_chain_sort/batch */
+#define GMF_MAX_LOOKBACK 1024       /* chaining predecessor window */
+
+/* ======================================================================== */
+/* Banded affine-gap Smith-Waterman with traceback                          */
+/* ======================================================================== */
+
+/* Integer scoring (the reference's defaults and every configuration it ships
+ * are integral; scores are exact int32).  x_drop <= 0 disables x-drop. */
+typedef struct {
+    int32_t match_score;      /* > 0 */
+    int32_t mismatch_penalty; /* >= 0, subtracted */
+    int32_t gap_open;         /* >= 0, cost of the first gap base */
+    int32_t gap_extend;       /* >= 0, cost of each further gap base */
+    int32_t x_drop;           /* stop when (best row max so far) - (row max) > x_drop */
+} gmf_sw_params;
+
+/* A batch of read/target pairs in CSR layout.  Base codes follow the
+ * reference alphabet: A=1 C=2 G=3 T=4 N=5, negative = padding; a query code
+ * matches a target code iff they are equal, >= 0 and != 5.
+ * Band slot d of query row i maps to target column
+ *     j = i + band_offset - half_band + d,   0 <= d < 2*half_band+1. */
+typedef struct {
+    int32_t n_pairs;
+    const int8_t* query;       /* concatenated query codes */
+    const int64_t* query_off;  /* n_pairs+1 offsets into query */
+    const int8_t* target;      /* concatenated target codes */
+    const int64_t* target_off; /* n_pairs+1 offsets into target */
+    const int32_t* half_band;  /* per pair, 0..GMF_MAX_HALF_BAND */
+    const int32_t* band_offset;/* per pair */
+    const int32_t* order;      /* optional processing order (a permutation of
+                                  0..n_pairs-1, e.g. longest first); NULL = 0..n-1.
+                                  It changes scheduling only, never results. */
+    int32_t max_half_band;     /* HOST value >= every half_band[p] (sizes shared memory) */
+} gmf_pairs;
+
+/* Per-pair outputs.  Ends are 1-based (0 when score == 0), starts 0-based,
+ * exactly as banded_affine_sw_batch / traceback_banded report them.  The
+ * CIGAR of pair p is cigar[cigar_start[p] .. + cigar_len[p]) as words
+ * (run_length << 4) | op with op 0 '=', 1 'X', 2 'I', 3 'D' (soft clips are
+ * added by the caller).  Pairs are packed densely in completion order; the
+ * device counter *cigar_used receives the total number of words. */
+typedef struct {
+    int32_t* score;
+    int32_t* query_end;
+    int32_t* target_end;
+    int32_t* query_start;        /* NULL allowed when cigar == NULL */
+    int32_t* target_start;       /* NULL allowed when cigar == NULL */
+    int32_t* op_counts;          /* 4 per pair (= X I D) or NULL */
+    uint32_t* cigar;             /* NULL = score/end only (no traceback) */
+    int64_t cigar_capacity;      /* words available in cigar */
+    int64_t* cigar_start;        /* per pair */
+    int32_t* cigar_len;          /* per pair, -1 if the pair overflowed cigar_capacity */
+    unsigned long long* cigar_used; /* one device word, written by the call */
+    int32_t* error_flags;        /* one device word: OR of GMF_SWF_* flags (written by the call) */
+} gmf_sw_results;
+
+#define GMF_SWF_WORKSPACE 1u /* a pair's traceback did not fit the workspace */
+#define GMF_SWF_CAPACITY 2u  /* cigar_capacity exceeded */
+
+/* Bytes of workspace gmf_banded_sw needs for a batch.  HOST arrays. */
+size_t gmf_banded_sw_workspace_bytes(int32_t n_pairs, const int32_t* query_len,
+                                     const int32_t* target_len, const int32_t* half_band,
+                                     int32_t with_traceback);
+
+/* Banded local alignment + traceback of every pair (one warp-group per pair,
+ * anti-diagonal lane pipeline, 4 traceback bits per cell).
+ * Replaces accel/cuda_kernels.py L504-566 and extension.py L78-302. */
+int gmf_banded_sw(const gmf_pairs* pairs, const gmf_sw_params* params,
+                  const gmf_sw_results* results, void* workspace, size_t workspace_bytes,
+                  gmf_stream_t stream);
+
+/* ======================================================================== */
+/* Anchor chaining                                                          */
+/* ======================================================================== */
+
+typedef struct {
+    int32_t max_lookback;           /* predecessors considered per anchor (>= 1) */
+    int32_t max_gap;                /* reject pairs separated by more than this */
+    int32_t min_chain_anchors;      /* chain filter */
+    int32_t max_chains;             /* chains kept per read (select) */
+    double min_chain_score;         /* chain filter */
+    double secondary_overlap;       /* select: drop chains overlapping the primary more */
+    double secondary_score_ratio;   /* select: drop chains below ratio * best */
+} gmf_chain_params;
+
+/* Chaining DP over rows that are already split by strand and sorted by
+ * (ref_end, read_end) -- chain_dp_numpy semantics, float64 exact:
+ *   f[i] = max(w_i, max_j ((f[j] + min(min(dq, dr), w_i)) - pen_lut[|dr-dq|]) [+ bonus])
+ * over j in [i - lookback, i) with 0 < dq, dr <= max_gap; the lowest j wins
+ * ties; the predecessor is taken only when strictly above w_i.
+ * pen_lut[g] must hold gap_open + gap_extend*g + log_coeff*log2(g+1) (0 at
+ * g = 0) for g = 0..max_gap, computed by the caller (numpy reproduces the
+ * reference's log2 exactly).  bonus: NULL or per anchor max_lookback values,
+ * column c for predecessor i - max_lookback + c.  parent is the row-local
+ * predecessor index or -1.  Replaces cuda_kernels.py L440-501. */
+int gmf_chain_dp(int32_t n_rows, const int64_t* row_off, const int32_t* read_end,
+                 const int32_t* ref_end, const double* weight, const double* bonus,
+                 int32_t max_lookback, int32_t max_gap, const double* pen_lut, int32_t lut_len,
+                 double* f, int32_t* parent, gmf_stream_t stream);
+
+/* Anchors of many reads in CSR layout, in each read's original order. */
+typedef struct {
+    int32_t n_reads;
+    const int64_t* read_off; /* n_reads+1 */
+    const int32_t* read_pos;
+    const int32_t* ref_pos;
+    const int32_t* length;
+    const int8_t* strand;    /* +1 / -1 (anything else is ignored, like for_strand) */
+} gmf_anchor_batch;
+
+/* Sorted layout (written by gmf_chain_sort): per read, the + strand anchors
+ * sorted by (ref_end, read_end, original index) followed by the - strand
+ * anchors sorted the same way, stored in the read's own range
+ * [read_off[r], read_off[r] + n_plus[r] + n_minus[r]). */
+typedef struct {
+    int32_t* perm;     /* sorted slot -> original index within the read */
+    int32_t* n_plus;   /* per read */
+    int32_t* n_minus;  /* per read */
+    int32_t* read_end; /* sorted read_pos + length */
+    int32_t* ref_end;  /* sorted ref_pos + length */
+} gmf_sorted_anchors;
+
+/* workspace: >= 256 + 24 * n_anchors bytes (gmf_chain_workspace_bytes is
+ * always enough); it holds the sort of reads too large for shared memory. */
+int gmf_chain_sort(const gmf_anchor_batch* anchors, const gmf_sorted_anchors* sorted,
+                   void* workspace, size_t workspace_bytes, gmf_stream_t stream);
+
+/* Per-read chain records, max_chains slots per read (slot k of read r at
+ * r*max_chains + k), ordered as select() returns them.  members: the
+ * original (within-read) anchor indices of the kept chains, back to back in
+ * slot order and in read order within a chain, stored in the read's own range
+ * [read_off[r], read_off[r+1]). */
+typedef struct {
+    int32_t* n_chains;   /* per read */
+    double* score;       /* per slot */
+    int32_t* strand;     /* per slot */
+    int32_t* span;       /* 4 per slot: read_start, read_end, ref_start, ref_end */
+    int32_t* is_primary; /* per slot */
+    int32_t* n_members;  /* per slot */
+    int32_t* members;    /* per anchor */
+} gmf_chain_results;
+
+size_t gmf_chain_workspace_bytes(int32_t n_reads, int64_t n_anchors);
+
+/* Full AffineChainer.chain for every read: strand split + sort, DP, chain
+ * peeling (_backtrack) and select.  sorted_weight / sorted_bonus are optional
+ * inputs in the layout gmf_chain_sort produces (hybrid mode: gated weights and
+ * graph / learned-transition bonus); NULL = weight is the anchor length, no
+ * bonus (fast mode).  When given, `sorted` must hold the output of a prior
+ * gmf_chain_sort on the same anchors; otherwise `sorted` may be NULL and the
+ * sort runs inside the call (in the workspace). */
+int gmf_chain_batch(const gmf_anchor_batch* anchors, const gmf_chain_params* params,
+                    const double* pen_lut, int32_t lut_len, const gmf_sorted_anchors* sorted,
+                    const double* sorted_weight, const double* sorted_bonus,
+                    const gmf_chain_results* results, void* workspace, size_t workspace_bytes,
+                    gmf_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GMF_ALIGN_H */

@@ -23,6 +23,9 @@ Fixtures:
   anchors of simulated HiFi reads.
 * ``extend_golden.npz`` -- ``ExtensionEngine.extend_chains`` on single-chain
   calls (window, band widening, soft clips).
+* ``hybrid_golden.pkl`` -- ``AffineChainer.chain`` with a ``ChainingContext``
+  (graph-distance oracle, backbone bias, neural seed scores with each AGNES
+  trust decision, learned transitions).
 """
 
 from __future__ import annotations
@@ -386,11 +389,75 @@ def make_extend(rng):
     print(f"extend_golden.npz: {len(results)} single-chain extensions")
 
 
+# --------------------------------------------------------------------------- #
+# hybrid-mode chain() (gated weights, graph + learned-transition bonus)
+# --------------------------------------------------------------------------- #
+def make_hybrid(rng):
+    from graphmambaformer.alignment.chaining import ChainingContext, GraphDistanceOracle
+
+    n_nodes = 60
+    edges = np.array([[i, i + 1] for i in range(n_nodes - 1)] + [[3, 10], [20, 35], [40, 41]]).T
+    oracle = GraphDistanceOracle(edges, n_nodes, max_hops=3)
+    backbone = np.zeros(n_nodes, dtype=bool)
+    backbone[::2] = True
+    reads = []
+    for r in range(16):
+        n_groups = int(rng.integers(1, 4))
+        rp, fp, ln, st, nid, sc = [], [], [], [], [], []
+        for g in range(n_groups):
+            k = int(rng.integers(3, 30))
+            start = int(rng.integers(0, 8000))
+            diag = int(rng.integers(0, 200_000))
+            pos = start + np.cumsum(rng.integers(8, 40, size=k))
+            rp.append(pos)
+            fp.append(pos + diag + np.cumsum(rng.integers(-3, 4, size=k)))
+            ln.append(rng.integers(12, 30, size=k))
+            st.append(np.full(k, 1 if rng.random() < 0.7 else -1, np.int8))
+            nid.append(np.where(rng.random(k) < 0.8, rng.integers(0, n_nodes, size=k), -1))
+            sc.append(rng.random(k).astype(np.float32) if r % 3 else np.full(k, np.nan, np.float32))
+        rp, fp, ln = (np.concatenate(x).astype(np.int64) for x in (rp, fp, ln))
+        a = AnchorSet.from_lists(rp, fp, ln, np.concatenate(st), node_id=np.concatenate(nid))
+        a.score = np.concatenate(sc)
+        if r % 4 == 1:  # decisive scores: high for group anchors, low for a few
+            a.score = np.where(rng.random(len(a)) < 0.8, 0.95, 0.05).astype(np.float32)
+        trust = [None, True, False, None][r % 4]
+        trans = None
+        if trust:
+            keys = [(int(a.read_pos[i]), int(a.ref_pos[i]), int(a.length[i]), int(a.strand[i]))
+                    for i in range(len(a))]
+            trans = {(keys[i], keys[i + 1]): float(rng.random()) for i in range(0, len(a) - 1, 2)}
+        ctx = ChainingContext(oracle=oracle if r % 2 == 0 else None,
+                              backbone=backbone if r % 3 != 2 else None,
+                              trust_neural=trust, learned_transitions=trans)
+        reads.append((a, ctx))
+    cfg = ChainingConfig(max_lookback=16, max_gap=5000)
+    chainer = AffineChainer(cfg, backend="torch", workers=1)
+    out = [chainer.chain(a, ctx, device="cpu") for a, ctx in reads]
+    import pickle
+
+    payload = dict(
+        edges=edges, n_nodes=n_nodes, backbone=backbone,
+        reads=[dict(read_pos=a.read_pos, ref_pos=a.ref_pos, length=a.length, strand=a.strand,
+                    node_id=a.node_id, score=a.score, use_oracle=ctx.oracle is not None,
+                    use_backbone=ctx.backbone is not None, trust=ctx.trust_neural,
+                    transitions=ctx.learned_transitions) for a, ctx in reads],
+        chains=[[dict(score=c.score, strand=c.strand, span=(c.read_start, c.read_end, c.ref_start,
+                                                             c.ref_end), primary=c.is_primary,
+                      members=np.asarray(c.anchor_idx)) for c in chains] for chains in out],
+        lookback=16,
+    )
+    with open(os.path.join(HERE, "hybrid_golden.pkl"), "wb") as fh:
+        pickle.dump(payload, fh, protocol=4)
+    print(f"hybrid_golden.pkl: {len(reads)} reads, {sum(len(c) for c in out)} chains")
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["sw", "chain", "extend"]
+    which = sys.argv[1:] or ["sw", "chain", "extend", "hybrid"]
     if "sw" in which:
         make_sw(np.random.default_rng(101))
     if "chain" in which:
         make_chain(np.random.default_rng(202))
     if "extend" in which:
         make_extend(np.random.default_rng(303))
+    if "hybrid" in which:
+        make_hybrid(np.random.default_rng(404))

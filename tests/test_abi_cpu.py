@@ -1,0 +1,117 @@
+"""C-ABI checks that need no GPU: the library loads, exports every function
+the public header declares, and the ctypes structures match the C layout."""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+import subprocess
+import sys
+
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "gmf_align.h")
+
+
+def declared_functions() -> list[str]:
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(gmf_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_function():
+    from graphmambaformer_b200 import _native
+
+    lib = _native.lib()
+    names = declared_functions()
+    assert "gmf_banded_sw" in names and "gmf_chain_batch" in names
+    for name in names:
+        assert hasattr(lib, name), name
+    # and the binding covers all of them with explicit signatures
+    assert set(names) == set(_native.exported_symbols())
+
+
+def test_status_strings_and_version():
+    from graphmambaformer_b200 import _native
+
+    assert _native.status_string(0) == "ok"
+    assert "workspace" in _native.status_string(_native.GMF_ERR_WORKSPACE)
+    assert _native.lib().gmf_version() >= 10000
+
+
+def test_workspace_helpers_are_host_only():
+    import numpy as np
+
+    from graphmambaformer_b200 import _native
+
+    q = np.array([150, 3000], np.int32)
+    t = np.array([214, 3064], np.int32)
+    hb = np.array([32, 100], np.int32)
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    b = _native.lib().gmf_banded_sw_workspace_bytes(2, p(q), p(t), p(hb), 1)
+    words = sum(((ql + 31) // 32) * ((2 * h + 1 + 7) // 8) * 32 + ql + tl + 1
+                for ql, tl, h in zip(q, t, hb))
+    assert b >= 256 + 4 * words
+    assert _native.lib().gmf_banded_sw_workspace_bytes(2, p(q), p(t), p(hb), 0) == 256
+    assert _native.lib().gmf_chain_workspace_bytes(10, 1000) > 1000 * 24
+
+
+_LAYOUT_C = r"""
+#include <stdio.h>
+#include <stddef.h>
+#include "gmf_align.h"
+#define P(T) printf(#T " %zu\n", sizeof(T))
+#define O(T, f) printf(#T "." #f " %zu\n", offsetof(T, f))
+int main(void) {
+  P(gmf_pairs); O(gmf_pairs, order); O(gmf_pairs, max_half_band);
+  P(gmf_sw_params); P(gmf_sw_results); O(gmf_sw_results, cigar_capacity); O(gmf_sw_results, error_flags);
+  P(gmf_chain_params); O(gmf_chain_params, min_chain_score);
+  P(gmf_anchor_batch); O(gmf_anchor_batch, strand);
+  P(gmf_sorted_anchors); P(gmf_chain_results); O(gmf_chain_results, members);
+  return 0;
+}
+"""
+
+
+def test_ctypes_structs_match_c_layout(tmp_path):
+    from graphmambaformer_b200 import _native as n
+
+    src = tmp_path / "layout.c"
+    exe = tmp_path / "layout"
+    src.write_text(_LAYOUT_C)
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(line.rsplit(" ", 1) for line in subprocess.check_output([str(exe)]).decode().splitlines())
+    want = {
+        "gmf_pairs": ctypes.sizeof(n.GmfPairs),
+        "gmf_pairs.order": n.GmfPairs.order.offset,
+        "gmf_pairs.max_half_band": n.GmfPairs.max_half_band.offset,
+        "gmf_sw_params": ctypes.sizeof(n.GmfSwParams),
+        "gmf_sw_results": ctypes.sizeof(n.GmfSwResults),
+        "gmf_sw_results.cigar_capacity": n.GmfSwResults.cigar_capacity.offset,
+        "gmf_sw_results.error_flags": n.GmfSwResults.error_flags.offset,
+        "gmf_chain_params": ctypes.sizeof(n.GmfChainParams),
+        "gmf_chain_params.min_chain_score": n.GmfChainParams.min_chain_score.offset,
+        "gmf_anchor_batch": ctypes.sizeof(n.GmfAnchorBatch),
+        "gmf_anchor_batch.strand": n.GmfAnchorBatch.strand.offset,
+        "gmf_sorted_anchors": ctypes.sizeof(n.GmfSortedAnchors),
+        "gmf_chain_results": ctypes.sizeof(n.GmfChainResults),
+        "gmf_chain_results.members": n.GmfChainResults.members.offset,
+    }
+    for k, v in want.items():
+        assert int(got[k]) == v, (k, got[k], v)
+
+
+def test_stages_refuse_to_run_without_a_gpu():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from graphmambaformer_b200.chaining import AffineChainer
+    from graphmambaformer_b200.types import AnchorSet
+
+    a = AnchorSet.from_lists([0, 20], [0, 20], [15, 15], [1, 1])
+    with pytest.raises(RuntimeError, match="CUDA"):
+        AffineChainer().chain(a)
