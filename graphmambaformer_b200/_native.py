@@ -124,6 +124,8 @@ _SIGNATURES = {
     "gmf_banded_sw_workspace_bytes": (c_size_t, [c_int32, c_void_p, c_void_p, c_void_p, c_int32]),
     "gmf_banded_sw": (c_int, [POINTER(GmfPairs), POINTER(GmfSwParams), POINTER(GmfSwResults),
                               c_void_p, c_size_t, c_void_p]),
+    "gmf_banded_sw_plain": (c_int, [POINTER(GmfPairs), POINTER(GmfSwParams), POINTER(GmfSwResults),
+                                    c_void_p, c_size_t, c_void_p]),
     "gmf_chain_dp": (c_int, [c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32,
                              c_int32, c_void_p, c_int32, c_void_p, c_void_p, c_void_p]),
     "gmf_chain_sort": (c_int, [POINTER(GmfAnchorBatch), POINTER(GmfSortedAnchors), c_void_p,

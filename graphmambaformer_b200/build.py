@@ -20,6 +20,8 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libgmf_align.so")
+PROBE_SRC = os.path.join(CSRC, "probe", "int_probe.cu")
+PROBE_LIB = os.path.join(LIBDIR, "libgmf_probe.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -42,7 +44,20 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def build_probe(force: bool = False) -> str:
+    """The integer-ALU throughput probe used as the SW roofline denominator."""
+    if not force and os.path.exists(PROBE_LIB) and os.path.getmtime(PROBE_LIB) >= os.path.getmtime(PROBE_SRC):
+        return PROBE_LIB
+    os.makedirs(LIBDIR, exist_ok=True)
+    tmp = PROBE_LIB + ".tmp"
+    subprocess.run([nvcc(), *ARCH, "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-cudart",
+                    "static", "-o", tmp, PROBE_SRC], check=True)
+    os.replace(tmp, PROBE_LIB)
+    return PROBE_LIB
+
+
 def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> str:
+    build_probe(force)
     if not force and not _stale():
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)

@@ -1,0 +1,267 @@
+// C ABI of the banded SW kernels: the batched form (device classifier + one
+// persistent, work-queue-driven kernel per pair class) and the plain form
+// (one warp per pair, int32, one launch).
+//
+// Batched form:
+//   1. sw_classify_kernel sorts the pairs (in the caller's processing order,
+//      e.g. longest first) into per-class lists in the workspace: int16x2 with
+//      8 / 16 / 32 lanes per pair chosen by band width, or int32 when a score
+//      could leave int16.  No host synchronisation: the compute kernels read
+//      the list lengths on the device.
+//   2. For each class a grid of (SMs x resident blocks) warps pulls pairs from
+//      the class list with an atomic head counter until the list is empty, so
+//      uneven pairs balance dynamically.
+// Results never depend on the class, the order or the batch: every path
+// computes the same integer DP and the same traceback decisions.
+
+#include <algorithm>
+
+#include "sw_common.cuh"
+
+namespace gmf {
+
+__host__ __device__ inline unsigned long long sw32_tb_words_api(int qlen, int W) {
+    const long long P = W + 1 > 64 ? W + 1 : 64;
+    const long long nstrips = (qlen + 31) / 32;
+    const long long last = (nstrips - 1) * P + 2 * ((qlen - 1) & 31) + W - 1;
+    return (unsigned long long)((last >> 3) + 1) * 32ull;
+}
+
+__host__ __device__ inline unsigned long long sw16_tb_words_api(int qlen, int W, int L) {
+    const long long V = 2 * L;
+    const long long P = (W + 2 > 4 * L) ? W + 2 : 4 * L;
+    const long long nstrips = (qlen + V - 1) / V;
+    const long long last = (nstrips - 1) * P + 2 * ((qlen - 1) % V) + W - 1;
+    return (unsigned long long)((last >> 2) + 1) * L;
+}
+
+// The int16x2 form is exact when no 16-bit value, sum or difference can wrap:
+// cells lie in [-(4*pmax + 2), smax] with smax = match * (min(qlen, tlen) + 1)
+// and pmax the largest penalty, and the traceback compares differences.
+__host__ __device__ inline int max_penalty(int mism, int go, int ge) {
+    const int m = mism > go ? mism : go;
+    return m > ge ? m : ge;
+}
+__host__ __device__ inline bool fits_int16(int qlen, int tlen, int match, int mism, int go, int ge) {
+    const long long smax = (long long)match * ((qlen < tlen ? qlen : tlen) + 1);
+    const int pmax = max_penalty(mism, go, ge);
+    return pmax <= 2048 && match <= 2048 && smax + 6LL * pmax + 64 <= 32767;
+}
+
+__host__ __device__ inline int sw_class(int qlen, int tlen, int hb, int match, int mism, int go, int ge) {
+    if (!fits_int16(qlen, tlen, match, mism, go, ge)) return CLS_I32;
+    const int W = 2 * hb + 1;
+    if (W <= 61) return CLS_I16_L8;
+    if (W <= 125) return CLS_I16_L16;
+    return CLS_I16_L32;
+}
+
+__global__ void sw_classify_kernel(SwArgs a) {
+    const int lane = threadIdx.x & 31;
+    for (int i0 = blockIdx.x * blockDim.x; i0 < a.n_pairs; i0 += gridDim.x * blockDim.x) {
+        const int idx = i0 + threadIdx.x;
+        int p = -1, cls = -1;
+        if (idx < a.n_pairs) {
+            p = a.order ? a.order[idx] : idx;
+            const int ql = (int)(a.q_off[p + 1] - a.q_off[p]);
+            const int tl = (int)(a.t_off[p + 1] - a.t_off[p]);
+            cls = sw_class(ql, tl, a.hb[p], a.match, a.mismatch, a.gap_open, a.gap_extend);
+        }
+        const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+        for (int c = 0; c < N_CLASSES; ++c) {
+            const unsigned b = __ballot_sync(FULL_MASK, cls == c);
+            if (!b) continue;
+            int base = 0;
+            const int leader = __ffs(b) - 1;
+            if (lane == leader) base = atomicAdd(&a.queue[N_CLASSES + c], __popc(b));
+            base = __shfl_sync(FULL_MASK, base, leader);
+            if (cls == c) a.lists[(size_t)c * a.n_pairs + base + __popc(b & lt)] = p;
+        }
+    }
+}
+
+static size_t round_up(size_t x, size_t m) { return (x + m - 1) / m * m; }
+
+static size_t queue_bytes(int n_pairs) {
+    return round_up(2 * N_CLASSES * sizeof(int32_t), 256) + round_up((size_t)N_CLASSES * n_pairs * 4, 256);
+}
+
+static int ring_entries(int d_max) {
+    int r = 1;
+    while (r < d_max + 1) r <<= 1;
+    return r;
+}
+
+static int check_common(const gmf_pairs* pairs, const gmf_sw_params* params, const gmf_sw_results* res) {
+    if (!pairs || !params || !res) return GMF_ERR_INVALID_ARGUMENT;
+    if (pairs->n_pairs < 0) return GMF_ERR_INVALID_ARGUMENT;
+    if (pairs->max_half_band < 0) return GMF_ERR_INVALID_ARGUMENT;
+    if (pairs->max_half_band > GMF_MAX_HALF_BAND) return GMF_ERR_LIMIT;
+    const int lim = 1 << 20;
+    if (params->match_score <= 0 || params->match_score > lim || params->mismatch_penalty < 0 ||
+        params->mismatch_penalty > lim || params->gap_open < 0 || params->gap_open > lim ||
+        params->gap_extend < 0 || params->gap_extend > lim)
+        return GMF_ERR_INVALID_ARGUMENT;
+    if (!res->score || !res->query_end || !res->target_end || !res->cigar_used || !res->error_flags)
+        return GMF_ERR_INVALID_ARGUMENT;
+    if (res->cigar && (!res->cigar_start || !res->cigar_len || res->cigar_capacity < 0))
+        return GMF_ERR_INVALID_ARGUMENT;
+    if (pairs->n_pairs > 0 && (!pairs->query || !pairs->query_off || !pairs->target ||
+                               !pairs->target_off || !pairs->half_band || !pairs->band_offset))
+        return GMF_ERR_INVALID_ARGUMENT;
+    return GMF_OK;
+}
+
+static void fill_args(SwArgs& a, const gmf_pairs* pairs, const gmf_sw_params* params,
+                      const gmf_sw_results* res) {
+    a.q = pairs->query;
+    a.q_off = pairs->query_off;
+    a.t = pairs->target;
+    a.t_off = pairs->target_off;
+    a.hb = pairs->half_band;
+    a.boff = pairs->band_offset;
+    a.order = pairs->order;
+    a.n_pairs = pairs->n_pairs;
+    a.match = params->match_score;
+    a.mismatch = params->mismatch_penalty;
+    a.gap_open = params->gap_open;
+    a.gap_extend = params->gap_extend;
+    a.x_drop = params->x_drop;
+    a.max_hb = pairs->max_half_band;
+    a.neg16 = -(2 * max_penalty(params->mismatch_penalty, params->gap_open, params->gap_extend) + 2);
+    a.score = res->score;
+    a.q_end = res->query_end;
+    a.t_end = res->target_end;
+    a.q_start = res->query_start;
+    a.t_start = res->target_start;
+    a.op_counts = res->op_counts;
+    a.cigar = res->cigar;
+    a.cigar_cap = res->cigar_capacity;
+    a.cigar_start = res->cigar_start;
+    a.cigar_len = res->cigar_len;
+    a.cigar_used = res->cigar_used;
+    a.err = res->error_flags;
+}
+
+static int e_mode_of(const gmf_sw_params* p) {
+    return p->gap_open > p->gap_extend ? 0 : (p->gap_open == p->gap_extend ? 1 : 2);
+}
+
+struct DevInfo {
+    int sms = 148;
+    int smem_optin = 227 * 1024;
+};
+
+static int dev_info(DevInfo& di) {
+    int dev = 0;
+    GMF_CUDA_TRY(cudaGetDevice(&dev));
+    GMF_CUDA_TRY(cudaDeviceGetAttribute(&di.sms, cudaDevAttrMultiProcessorCount, dev));
+    GMF_CUDA_TRY(cudaDeviceGetAttribute(&di.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    return GMF_OK;
+}
+
+// Warps per block that fit the per-warp shared memory.
+static int warps_per_block(size_t per_warp, const DevInfo& di) {
+    int wpb = 4;
+    while (wpb > 1 && per_warp * wpb > (size_t)di.smem_optin) --wpb;
+    return per_warp > (size_t)di.smem_optin ? 0 : wpb;
+}
+
+}  // namespace gmf
+
+using namespace gmf;
+
+extern "C" size_t gmf_banded_sw_workspace_bytes(int32_t n_pairs, const int32_t* qlen,
+                                                const int32_t* tlen, const int32_t* half_band,
+                                                int32_t with_traceback) {
+    size_t words = 0;
+    if (n_pairs > 0 && qlen && tlen && half_band) {
+        for (int32_t p = 0; p < n_pairs; ++p) {
+            const int ql = std::max(qlen[p], 0), tl = std::max(tlen[p], 0);
+            const int W = 2 * std::max(half_band[p], 0) + 1;
+            words += 2 * (size_t)ql + 8;  // row maxima (x-drop) + alignment padding
+            if (with_traceback && ql > 0) {
+                // the larger of the int32 and int16x2 layouts, whichever class the pair gets
+                unsigned long long tb = sw32_tb_words_api(ql, W);
+                for (int L = 8; L <= 32; L <<= 1) tb = std::max(tb, sw16_tb_words_api(ql, W, L));
+                words += tb + (size_t)ql + tl + 1;
+            }
+        }
+    }
+    return 256 + queue_bytes(std::max(n_pairs, 0)) + round_up(words * 4, 256);
+}
+
+static int sw_prepare(const gmf_pairs* pairs, const gmf_sw_params* params, const gmf_sw_results* res,
+                      void* workspace, size_t workspace_bytes, cudaStream_t stream, SwArgs& a) {
+    GMF_TRY(check_common(pairs, params, res));
+    const size_t qb = queue_bytes(pairs->n_pairs);
+    if (!workspace || workspace_bytes < 256 + qb) return GMF_ERR_WORKSPACE;
+    GMF_TRY(bind_stream_device(stream));
+    GMF_CUDA_TRY(cudaMemsetAsync(workspace, 0, 256 + round_up(2 * N_CLASSES * sizeof(int32_t), 256), stream));
+    GMF_CUDA_TRY(cudaMemsetAsync(res->cigar_used, 0, sizeof(unsigned long long), stream));
+    GMF_CUDA_TRY(cudaMemsetAsync(res->error_flags, 0, sizeof(int32_t), stream));
+    fill_args(a, pairs, params, res);
+    char* w = (char*)workspace;
+    a.counters = (unsigned long long*)w;
+    a.queue = (int32_t*)(w + 256);
+    a.lists = (int32_t*)(w + 256 + round_up(2 * N_CLASSES * sizeof(int32_t), 256));
+    a.pool = (uint32_t*)(w + 256 + qb);
+    a.pool_cap = (workspace_bytes - 256 - qb) / 4;
+    return GMF_OK;
+}
+
+extern "C" int gmf_banded_sw(const gmf_pairs* pairs, const gmf_sw_params* params,
+                             const gmf_sw_results* res, void* workspace, size_t workspace_bytes,
+                             gmf_stream_t stream_) {
+    const cudaStream_t stream = (cudaStream_t)stream_;
+    SwArgs a;
+    GMF_TRY(sw_prepare(pairs, params, res, workspace, workspace_bytes, stream, a));
+    if (pairs->n_pairs == 0) return GMF_OK;
+    DevInfo di;
+    GMF_TRY(dev_info(di));
+    const bool tb = res->cigar != nullptr;
+    const bool xd = params->x_drop > 0;
+    const int em = e_mode_of(params);
+
+    const int cls_blocks = std::min((pairs->n_pairs + 255) / 256, di.sms * 4);
+    sw_classify_kernel<<<cls_blocks, 256, 0, stream>>>(a);
+    GMF_CUDA_TRY(cudaGetLastError());
+
+    const int Wmax = 2 * pairs->max_half_band + 1;
+    // int16x2 classes (a class only ever holds pairs up to its own band limit)
+    const int cls_wmax[3] = {std::min(Wmax, 61), std::min(Wmax, 125), Wmax};
+    const int lanes[3] = {8, 16, 32};
+    for (int c = 0; c < 3; ++c) {
+        const int L = lanes[c];
+        SwArgs ac = a;
+        ac.ring = ring_entries(std::max(0, cls_wmax[c] + 2 - 4 * L));
+        const int wpb = warps_per_block((size_t)sw16_smem_per_warp(c, ac.ring), di);
+        if (wpb == 0) return GMF_ERR_LIMIT;
+        const int grid = di.sms * std::max(1, 16 / wpb);
+        GMF_TRY(launch_sw16(ac, c, tb, xd, em, grid, wpb, stream));
+    }
+    SwArgs a32 = a;
+    a32.ring = ring_entries(std::max(64, Wmax + 1) - 64);
+    const int wpb = warps_per_block((size_t)sw32_smem_per_warp(a32.ring), di);
+    if (wpb == 0) return GMF_ERR_LIMIT;
+    return launch_sw32(a32, tb, xd, em, true, di.sms * std::max(1, 12 / wpb), wpb, stream);
+}
+
+extern "C" int gmf_banded_sw_plain(const gmf_pairs* pairs, const gmf_sw_params* params,
+                                   const gmf_sw_results* res, void* workspace, size_t workspace_bytes,
+                                   gmf_stream_t stream_) {
+    const cudaStream_t stream = (cudaStream_t)stream_;
+    SwArgs a;
+    GMF_TRY(sw_prepare(pairs, params, res, workspace, workspace_bytes, stream, a));
+    if (pairs->n_pairs == 0) return GMF_OK;
+    DevInfo di;
+    GMF_TRY(dev_info(di));
+    const int Wmax = 2 * pairs->max_half_band + 1;
+    a.ring = ring_entries(std::max(64, Wmax + 1) - 64);
+    const int wpb = warps_per_block((size_t)sw32_smem_per_warp(a.ring), di);
+    if (wpb == 0) return GMF_ERR_LIMIT;
+    const int grid = (pairs->n_pairs + wpb - 1) / wpb;
+    return launch_sw32(a, res->cigar != nullptr, params->x_drop > 0, e_mode_of(params), false, grid,
+                       wpb, stream);
+}

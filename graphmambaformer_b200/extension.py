@@ -169,10 +169,20 @@ def workspace_bytes(dp: DevicePairs, traceback: bool) -> int:
         dp.n, np_ptr(dp.h_qlen), np_ptr(dp.h_tlen), np_ptr(dp.h_hb), 1 if traceback else 0))
 
 
+FORMS = ("batched", "plain")
+
+
 def launch_banded_sw(dp: DevicePairs, params: _native.GmfSwParams, traceback: bool = True,
                      out: Optional[SWOutputs] = None, workspace: Optional[torch.Tensor] = None,
-                     stream: Optional[torch.cuda.Stream] = None) -> SWOutputs:
-    """Enqueue gmf_banded_sw on ``stream`` (default: the current stream)."""
+                     stream: Optional[torch.cuda.Stream] = None, form: str = "batched") -> SWOutputs:
+    """Enqueue the banded SW on ``stream`` (default: the current stream).
+
+    ``form="batched"`` (default) is gmf_banded_sw: device classifier, int16x2
+    cells where scores fit, persistent work-queue kernels.  ``form="plain"``
+    is gmf_banded_sw_plain: one warp per pair, int32 cells.  Both give
+    identical results."""
+    if form not in FORMS:
+        raise ValueError(f"form must be one of {FORMS}")
     out = out or SWOutputs.allocate(dp, traceback)
     need = workspace_bytes(dp, traceback)
     ws = workspace if workspace is not None and workspace.numel() >= need else WORKSPACE.get(dp.device, need)
@@ -185,9 +195,10 @@ def launch_banded_sw(dp: DevicePairs, params: _native.GmfSwParams, traceback: bo
         ptr(out.target_start), ptr(out.op_counts), ptr(out.cigar),
         out.cigar.numel() if out.cigar is not None else 0, ptr(out.cigar_start), ptr(out.cigar_len),
         ptr(out.cigar_used), ptr(out.error_flags))
-    st = _native.lib().gmf_banded_sw(ctypes.byref(pairs), ctypes.byref(params), ctypes.byref(res),
-                                     ctypes.c_void_p(ws.data_ptr()), ws.numel(), ctypes.c_void_p(sp))
-    _native.check("gmf_banded_sw", st)
+    fn = _native.lib().gmf_banded_sw if form == "batched" else _native.lib().gmf_banded_sw_plain
+    st = fn(ctypes.byref(pairs), ctypes.byref(params), ctypes.byref(res),
+            ctypes.c_void_p(ws.data_ptr()), ws.numel(), ctypes.c_void_p(sp))
+    _native.check("gmf_banded_sw" if form == "batched" else "gmf_banded_sw_plain", st)
     return out
 
 
@@ -246,11 +257,11 @@ def fetch(out: SWOutputs, n: int) -> SWResult:
 
 
 def align_pairs(pairs: PairSet, params: Optional[_native.GmfSwParams] = None, traceback: bool = True,
-                device=None, order: Optional[np.ndarray] = None) -> SWResult:
+                device=None, order: Optional[np.ndarray] = None, form: str = "batched") -> SWResult:
     """Host pairs in, host alignments out (upload, one launch, download)."""
     params = params or sw_params()
     dp = upload_pairs(pairs, device, order=order)
-    out = launch_banded_sw(dp, params, traceback)
+    out = launch_banded_sw(dp, params, traceback, form=form)
     return fetch(out, dp.n)
 
 

@@ -71,8 +71,9 @@ class ExtensionSession:
 
     def __init__(self, device=None, match_score=2.0, mismatch_penalty=4.0, gap_open=6.0,
                  gap_extend=2.0, x_drop=0.0, traceback: bool = True,
-                 stream: Optional[torch.cuda.Stream] = None):
+                 stream: Optional[torch.cuda.Stream] = None, form: str = "batched"):
         self.device = require_cuda(device)
+        self.form = form
         self.params = sw_params(match_score, mismatch_penalty, gap_open, gap_extend, x_drop)
         self.traceback = traceback
         self.stream = stream or torch.cuda.Stream(self.device)
@@ -124,9 +125,9 @@ class ExtensionSession:
             out["clen"].data_ptr() if tb else None, used.data_ptr(), err.data_ptr())
         sp = int(s.cuda_stream)
         bind(self.device, sp)
-        st = _native.lib().gmf_banded_sw(ctypes.byref(pairs_c), ctypes.byref(self.params),
-                                         ctypes.byref(res_c), ctypes.c_void_p(ws.data_ptr()),
-                                         ws.numel(), ctypes.c_void_p(sp))
+        fn = _native.lib().gmf_banded_sw if self.form == "batched" else _native.lib().gmf_banded_sw_plain
+        st = fn(ctypes.byref(pairs_c), ctypes.byref(self.params), ctypes.byref(res_c),
+                ctypes.c_void_p(ws.data_ptr()), ws.numel(), ctypes.c_void_p(sp))
         _native.check("gmf_banded_sw", st)
         dl = self.buf.download
         names = ["score", "qe", "te"] + (["qs", "ts", "clen"] if tb else [])

@@ -125,12 +125,22 @@ size_t gmf_banded_sw_workspace_bytes(int32_t n_pairs, const int32_t* query_len,
                                      const int32_t* target_len, const int32_t* half_band,
                                      int32_t with_traceback);
 
-/* Banded local alignment + traceback of every pair (one warp-group per pair,
- * anti-diagonal lane pipeline, 4 traceback bits per cell).
+/* Banded local alignment + traceback of every pair, batched form: a device
+ * classifier puts each pair in a work list (int16x2 cells with 8/16/32 lanes
+ * per pair by band width, or int32 cells when a score could leave int16) and
+ * one persistent kernel per list pulls pairs until it is empty.  Results are
+ * identical to gmf_banded_sw_plain for every pair.
  * Replaces accel/cuda_kernels.py L504-566 and extension.py L78-302. */
 int gmf_banded_sw(const gmf_pairs* pairs, const gmf_sw_params* params,
                   const gmf_sw_results* results, void* workspace, size_t workspace_bytes,
                   gmf_stream_t stream);
+
+/* Plain per-batch form: one warp per pair in input order, int32 cells, one
+ * launch (the baseline the batched form is measured against).  Same inputs,
+ * outputs and workspace as gmf_banded_sw. */
+int gmf_banded_sw_plain(const gmf_pairs* pairs, const gmf_sw_params* params,
+                        const gmf_sw_results* results, void* workspace, size_t workspace_bytes,
+                        gmf_stream_t stream);
 
 /* ======================================================================== */
 /* Anchor chaining                                                          */

@@ -52,10 +52,12 @@ def test_workspace_helpers_are_host_only():
     hb = np.array([32, 100], np.int32)
     p = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
     b = _native.lib().gmf_banded_sw_workspace_bytes(2, p(q), p(t), p(hb), 1)
-    words = sum(((ql + 31) // 32) * ((2 * h + 1 + 7) // 8) * 32 + ql + tl + 1
-                for ql, tl, h in zip(q, t, hb))
-    assert b >= 256 + 4 * words
-    assert _native.lib().gmf_banded_sw_workspace_bytes(2, p(q), p(t), p(hb), 0) == 256
+    # traceback: one 4-bit code per pipeline step (>= one per DP cell), the
+    # per-row maxima and the CIGAR-run scratch
+    cells = sum(int(ql) * (2 * int(h) + 1) for ql, h in zip(q, hb))
+    assert b >= 256 + cells // 2 + 4 * sum(2 * int(ql) + int(ql) + int(tl) + 1 for ql, tl in zip(q, t))
+    no_tb = _native.lib().gmf_banded_sw_workspace_bytes(2, p(q), p(t), p(hb), 0)
+    assert 256 + 8 * int(q.sum()) <= no_tb < b
     assert _native.lib().gmf_chain_workspace_bytes(10, 1000) > 1000 * 24
 
 

@@ -19,10 +19,11 @@ def ext():
     return extension
 
 
-def test_sw_matches_reference_golden(ext):
+@pytest.mark.parametrize("form", ["batched", "plain"])
+def test_sw_matches_reference_golden(ext, form):
     n = 0
     for p, idx, ps, g in golden_sw_pairs():
-        res = ext.align_pairs(ps, ext.sw_params(*p), traceback=True)
+        res = ext.align_pairs(ps, ext.sw_params(*p), traceback=True, form=form)
         for k, b in enumerate(idx):
             tag = str(g["tag"][b])
             assert res.score[k] == g["score"][b], (tag, b, res.score[k], g["score"][b])
@@ -66,7 +67,7 @@ def test_sw_matches_oracle_mixed_profiles(ext):
 
     ps = synth.extension_pairs_mixed(n_pairs=400, seed=7, ref_len=2_000_000, max_len=4000,
                                      log_mean=6.5, log_sigma=0.8)
-    for params in ((2, 4, 4, 2, 0), (2, 4, 6, 2, 600), (1, 3, 5, 1, 40)):
+    for params in ((2, 4, 4, 2, 0), (2, 4, 6, 2, 600), (1, 3, 5, 1, 40), (3, 2, 2, 2, 25), (2, 5, 1, 3, 0)):
         res = ext.align_pairs(ps, ext.sw_params(*params))
         want = oracle.sw_batch([ps.q(b) for b in range(len(ps))], [ps.t(b) for b in range(len(ps))],
                                ps.half_band, ps.band_offset, *params, threads=8)
@@ -172,3 +173,48 @@ def test_rejects_band_beyond_limit(ext):
         ext.align_pairs(ps, ext.sw_params())
     with pytest.raises(ValueError):
         ext.sw_params(2.5, 4, 6, 2, 0)
+
+
+def test_batched_and_plain_forms_agree_on_every_class(ext):
+    """int16x2 with 8/16/32 lanes, int32 (scores beyond int16), x-drop on and
+    off: the batched form equals the plain int32 form field for field."""
+    from graphmambaformer_b200 import synth
+
+    rng = np.random.default_rng(21)
+    ref = synth.random_reference(400_000, rng)
+    qs, ts, hbs = [], [], []
+    for L, hb in ((80, 5), (300, 20), (900, 45), (600, 90), (2000, 200), (17_000, 40), (300, 0), (50, 300)):
+        for _ in range(6):
+            s = int(rng.integers(500, 350_000 - L))
+            qs.append(synth.apply_errors(ref[s: s + L], synth.ONT, rng))
+            ts.append(ref[s - 100: s + L + 100])
+            hbs.append(hb)
+    ps = synth.PairSet.from_lists(qs, ts, np.array(hbs, np.int32), 100)
+    for params in ((2, 4, 4, 2, 0), (2, 4, 6, 2, 600), (2, 4, 4, 4, 30)):
+        a = ext.align_pairs(ps, ext.sw_params(*params), form="batched")
+        b = ext.align_pairs(ps, ext.sw_params(*params), form="plain")
+        assert np.array_equal(a.score, b.score), params
+        assert np.array_equal(a.query_end, b.query_end) and np.array_equal(a.target_end, b.target_end)
+        assert np.array_equal(a.query_start, b.query_start) and np.array_equal(a.target_start, b.target_start)
+        assert np.array_equal(a.op_counts, b.op_counts)
+        assert all(a.cigar(k) == b.cigar(k) for k in range(len(ps))), params
+
+
+def test_int16_eligibility_boundary(ext):
+    """Identical sequences whose scores sit just inside and just outside the
+    int16 range of the batched form (16-bit cells up to ~32.6k) agree with the
+    plain int32 form and with the closed-form score."""
+    from graphmambaformer_b200 import synth
+
+    rng = np.random.default_rng(77)
+    qs, ts = [], []
+    for n in (16_300, 16_330, 16_340, 16_400):
+        s = synth.random_reference(n, rng)
+        qs.append(s)
+        ts.append(s.copy())
+    ps = synth.PairSet.from_lists(qs, ts, 8, 0)
+    a = ext.align_pairs(ps, ext.sw_params(2, 4, 6, 2, 0), form="batched")
+    b = ext.align_pairs(ps, ext.sw_params(2, 4, 6, 2, 0), form="plain")
+    assert list(a.score) == [2 * len(x) for x in qs]
+    assert np.array_equal(a.score, b.score) and np.array_equal(a.query_end, b.query_end)
+    assert all(a.cigar(k) == [("=", len(qs[k]))] for k in range(len(qs)))
