@@ -90,6 +90,8 @@ struct SortArgs {
     unsigned long long* gkey;  // workspace: 2 * n_anchors keys (large reads)
     int* gidx;                 // workspace: 2 * n_anchors indices
     int smem_elems;
+    int64_t cap;               // anchors the sorted outputs can hold (-1: caller-sized)
+    int64_t key_cap;           // anchors gkey / gidx cover (2 entries each)
     int* err;
 };
 
@@ -101,11 +103,13 @@ __global__ void __launch_bounds__(256) chain_sort_kernel(SortArgs a) {
     const int n = (int)(a.read_off[r + 1] - a0);
     __shared__ int cnt[2];
     if (threadIdx.x < 2) cnt[threadIdx.x] = 0;
-    if (n > GMF_MAX_READ_ANCHORS) {
+    if (n > GMF_MAX_READ_ANCHORS || (a.cap >= 0 && a.read_off[r + 1] > a.cap)) {
+        // too many anchors for one read, or beyond what the workspace holds:
+        // the read gets no sorted anchors (so no chains) and the error word says why
         if (threadIdx.x == 0) {
             a.n_plus[r] = 0;
             a.n_minus[r] = 0;
-            if (a.err) atomicOr(a.err, 1);
+            if (a.err) atomicOr(a.err, n > GMF_MAX_READ_ANCHORS ? 1 : 4);
         }
         return;
     }
@@ -115,7 +119,7 @@ __global__ void __launch_bounds__(256) chain_sort_kernel(SortArgs a) {
     if (np2 <= a.smem_elems) {
         key = sm_keys;
         idx = reinterpret_cast<int*>(sm_keys + a.smem_elems);
-    } else if (a.gkey && a.gidx) {
+    } else if (a.gkey && a.gidx && 2 * a0 + np2 <= 2 * a.key_cap) {
         key = a.gkey + 2 * a0;
         idx = a.gidx + 2 * a0;
     } else {
@@ -181,6 +185,7 @@ struct DpArgs {
     double* f;
     int32_t* parent;
     int32_t ring;            // ring entries per warp (power of two > lookback)
+    int64_t cap;             // reads mode: anchors f / parent hold (-1: caller-sized)
 };
 
 __device__ __forceinline__ void seg_range(const DpArgs& a, int s, int64_t& start, int& n) {
@@ -197,6 +202,7 @@ __device__ __forceinline__ void seg_range(const DpArgs& a, int s, int64_t& start
             start = a0 + a.n_plus[r];
             n = a.n_minus[r];
         }
+        if (a.cap >= 0 && start + n > a.cap) n = 0;  // beyond the workspace: skipped
     }
 }
 
@@ -308,6 +314,7 @@ struct PeelArgs {
     int8_t* c_strand;
     int8_t* claimed;           // per anchor
     int smem_elems;
+    int64_t cap;               // anchors the workspace arrays hold
     // results
     int32_t* n_chains;
     double* score;
@@ -331,6 +338,10 @@ __global__ void __launch_bounds__(256) chain_peel_kernel(PeelArgs a) {
     }
     const int np = a.n_plus[r], nm = a.n_minus[r];
     const int n_sorted = np + nm;
+    if (a0 + n_sorted > a.cap) {  // beyond the workspace (the sort reported it): no chains
+        if (threadIdx.x == 0) a.n_chains[r] = 0;
+        return;
+    }
     // claimed flags reuse the tie-index array after the sort (one byte each)
     for (int seg = 0; seg < 2; ++seg) {
         const int n = seg == 0 ? np : nm;
@@ -494,7 +505,7 @@ int sort_smem_elems() { return 8192; }  // 8192 * 12 B = 96 KB
 size_t sort_smem_bytes(int elems) { return (size_t)elems * (sizeof(unsigned long long) + sizeof(int)); }
 
 int launch_sort(const gmf_anchor_batch* an, const gmf_sorted_anchors* so, unsigned long long* gkey,
-                int* gidx, int* err, cudaStream_t stream) {
+                int* gidx, int64_t cap, int64_t key_cap, int* err, cudaStream_t stream) {
     SortArgs s;
     s.n_reads = an->n_reads;
     s.read_off = an->read_off;
@@ -510,6 +521,8 @@ int launch_sort(const gmf_anchor_batch* an, const gmf_sorted_anchors* so, unsign
     s.gkey = gkey;
     s.gidx = gidx;
     s.smem_elems = sort_smem_elems();
+    s.cap = cap;
+    s.key_cap = key_cap;
     s.err = err;
     const size_t smem = sort_smem_bytes(s.smem_elems);
     GMF_CUDA_TRY(cudaFuncSetAttribute(chain_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -585,7 +598,7 @@ extern "C" int gmf_chain_sort(const gmf_anchor_batch* an, const gmf_sorted_ancho
         gkey = nullptr;
     }
     GMF_CUDA_TRY(cudaMemsetAsync(err, 0, 4, (cudaStream_t)stream));
-    return launch_sort(an, so, gkey, gidx, err, (cudaStream_t)stream);
+    return launch_sort(an, so, gkey, gidx, -1, (int64_t)A, err, (cudaStream_t)stream);
 }
 
 extern "C" size_t gmf_chain_workspace_bytes(int32_t n_reads, int64_t n_anchors) {
@@ -674,7 +687,7 @@ extern "C" int gmf_chain_batch(const gmf_anchor_batch* an, const gmf_chain_param
     GMF_CUDA_TRY(cudaMemsetAsync(err, 0, 256, stream));
     int st;
     if (!sorted_in) {
-        st = launch_sort(an, &so, gkey, gidx, err, stream);
+        st = launch_sort(an, &so, gkey, gidx, (int64_t)A, (int64_t)A, err, stream);
         if (st) return st;
     }
     DpArgs d{};
@@ -693,6 +706,7 @@ extern "C" int gmf_chain_batch(const gmf_anchor_batch* an, const gmf_chain_param
     d.lut_len = lut_len;
     d.f = f;
     d.parent = parent;
+    d.cap = (int64_t)A;
     st = launch_dp(d, 2 * an->n_reads, stream);
     if (st) return st;
 
@@ -721,6 +735,7 @@ extern "C" int gmf_chain_batch(const gmf_anchor_batch* an, const gmf_chain_param
     k.c_strand = c_strand;
     k.claimed = c_strand + A;
     k.smem_elems = sort_smem_elems();
+    k.cap = (int64_t)A;
     k.n_chains = res->n_chains;
     k.score = res->score;
     k.strand = res->strand;
