@@ -28,6 +28,7 @@ GMF_SWF_CAPACITY = 2
 MAX_HALF_BAND = 4096
 MAX_READ_ANCHORS = 16384
 MAX_LOOKBACK = 1024
+CHAIN_NOALLOC_SCRATCH_BYTES = 32 << 20
 
 
 class GmfPairs(Structure):
@@ -134,6 +135,8 @@ _SIGNATURES = {
     "gmf_chain_batch": (c_int, [POINTER(GmfAnchorBatch), POINTER(GmfChainParams), c_void_p,
                                 c_int32, POINTER(GmfSortedAnchors), c_void_p, c_void_p,
                                 POINTER(GmfChainResults), c_void_p, c_size_t, c_void_p]),
+    "gmf_chain_batch_noalloc": (c_int, [POINTER(GmfAnchorBatch), POINTER(GmfChainParams), c_void_p,
+                                        c_int32, c_int64, POINTER(GmfChainResults), c_void_p]),
 }
 
 _lib = None

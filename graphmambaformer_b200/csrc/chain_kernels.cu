@@ -22,6 +22,7 @@
 #include <float.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "gmf_common.cuh"
 
@@ -748,4 +749,54 @@ extern "C" int gmf_chain_batch(const gmf_anchor_batch* an, const gmf_chain_param
                                       (int)smem));
     chain_peel_kernel<<<an->n_reads, 256, smem, stream>>>(k);
     return cuda_status(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free chaining: the scratch is a fixed array of this library.
+// ---------------------------------------------------------------------------
+
+// Scratch of gmf_chain_batch_noalloc, one copy per GPU that loads the library.
+// Host code must not pass `g_chain_scratch` itself to a kernel (on the host it
+// names a stand-in, not device memory); it uses the address looked up below.
+static __device__ __align__(256) unsigned char g_chain_scratch[GMF_CHAIN_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int kMaxScratchDevices = 64;
+std::mutex g_scratch_mu;
+void* g_scratch_addr[kMaxScratchDevices] = {};
+
+// Device address of g_chain_scratch on the current device, looked up once per
+// device (the lookup may load this library's module on that device).
+int chain_scratch_address(void** out) {
+    int dev = 0;
+    GMF_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxScratchDevices) return GMF_ERR_LIMIT;
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (!g_scratch_addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_chain_scratch);
+        if (e != cudaSuccess || !p) return GMF_ERR_CUDA;
+        g_scratch_addr[dev] = p;
+    }
+    *out = g_scratch_addr[dev];
+    return GMF_OK;
+}
+
+}  // namespace
+
+extern "C" int gmf_chain_batch_noalloc(const gmf_anchor_batch* an, const gmf_chain_params* cp,
+                                       const double* pen_lut, int32_t lut_len, int64_t n_anchors,
+                                       const gmf_chain_results* res, gmf_stream_t stream) {
+    if (!an || !cp || !res || an->n_reads < 0 || n_anchors < 0) return GMF_ERR_INVALID_ARGUMENT;
+    const size_t need = gmf_chain_workspace_bytes(an->n_reads, n_anchors);
+    if (need > GMF_CHAIN_NOALLOC_SCRATCH_BYTES) return GMF_ERR_LIMIT;
+    if (an->n_reads == 0) return GMF_OK;
+    GMF_TRY(bind_stream_device((cudaStream_t)stream));
+    void* scratch = nullptr;
+    GMF_TRY(chain_scratch_address(&scratch));
+    // gmf_chain_batch clears the error word itself; every other scratch array
+    // is written before it is read (sort keys, DP values, claimed flags)
+    return gmf_chain_batch(an, cp, pen_lut, lut_len, nullptr, nullptr, nullptr, res, scratch, need,
+                           stream);
 }

@@ -228,6 +228,34 @@ int gmf_chain_batch(const gmf_anchor_batch* anchors, const gmf_chain_params* par
                     const gmf_chain_results* results, void* workspace, size_t workspace_bytes,
                     gmf_stream_t stream);
 
+/* ======================================================================== */
+/* Chaining without device allocation                                       */
+/* ======================================================================== */
+
+/* Scratch held by gmf_chain_batch_noalloc: a fixed array inside this library,
+ * present on every GPU that loads it, for as long as the process runs. */
+#define GMF_CHAIN_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
+
+/* gmf_chain_batch in fast mode (weight = anchor length, no bonus) for callers
+ * that cannot allocate device memory: a plugin host that hands over only its
+ * input and output buffers, a process whose HBM is all held by a pool it does
+ * not control, or a latency-bound loop that must not call cudaMalloc/cudaFree
+ * (they synchronise the device).  Inputs and outputs are the caller's, as in
+ * gmf_chain_batch; the scratch is the library's fixed array, so the call takes
+ * no workspace.  There is no counterpart in the reference.
+ *   n_anchors  HOST value: total anchors of the batch (read_off[n_reads]).
+ *              GMF_ERR_LIMIT when gmf_chain_workspace_bytes(n_reads, n_anchors)
+ *              exceeds GMF_CHAIN_NOALLOC_SCRATCH_BYTES (about 390,000 anchors).
+ *   The first call on a device looks up the array's device address (once per
+ *   device, under a lock), so make that first call before any stream capture.
+ *   Every call shares the one array per device: calls whose work overlaps on
+ *   the GPU (other streams, other threads) race and corrupt each other's
+ *   results; serialise them, e.g. on one stream.  The array keeps the last
+ *   call's contents; each call clears the parts that must start at zero. */
+int gmf_chain_batch_noalloc(const gmf_anchor_batch* anchors, const gmf_chain_params* params,
+                            const double* pen_lut, int32_t lut_len, int64_t n_anchors,
+                            const gmf_chain_results* results, gmf_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
