@@ -7,6 +7,8 @@
 //   kind 2: packed 16x2: x = vmax(vadd(x, a), y); y = ...  8 lane-ops (2 halves) per step
 //   kinds 3-6 time single intrinsics (16x2 compares, DPX max forms, byte
 //   permute / funnel shift) so their cost relative to one int32 op is known
+//   kinds 7-9 time the unsigned 16x2 forms (max, min, three-way max, DPX
+//   add-max) the biased-unsigned SW cells use
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -42,6 +44,15 @@ __global__ void int_probe_kernel(int iters, int a, int b, int* out) {
                 bool p0, p1;
                 x[k] = (int)__vibmax_s16x2((unsigned)x[k], (unsigned)y[k], &p0, &p1);
                 y[k] = y[k] + (p0 ? a : b) + (p1 ? b : a);
+            } else if (KIND == 7) {  // unsigned 16x2 max / min
+                x[k] = (int)__vmaxu2((unsigned)x[k], (unsigned)y[k]) + a;
+                y[k] = (int)__vminu2((unsigned)y[k], (unsigned)x[k]) ^ b;
+            } else if (KIND == 8) {  // unsigned 16x2 three-way max + packed sub
+                x[k] = (int)__vimax3_u16x2((unsigned)x[k], (unsigned)y[k], (unsigned)a);
+                y[k] = (int)__vsub2((unsigned)y[k], (unsigned)x[k]);
+            } else if (KIND == 9) {  // DPX unsigned 16x2 add-max
+                x[k] = (int)__viaddmax_u16x2((unsigned)x[k], (unsigned)a, (unsigned)y[k]);
+                y[k] = (int)__viaddmax_u16x2((unsigned)y[k], (unsigned)b, (unsigned)x[k]);
             } else {  // byte permute + funnel shift (exchange and bit packing)
                 x[k] = (int)__byte_perm((unsigned)x[k], (unsigned)y[k], 0x5432) + a;
                 y[k] = (int)__funnelshift_r((unsigned)y[k], (unsigned)x[k], 8);
@@ -66,7 +77,10 @@ extern "C" int gmf_probe_int(int kind, int blocks, int threads, int iters, int* 
         case 3: int_probe_kernel<3><<<blocks, threads, 0, s>>>(iters, 0x00030003, 0x00050005, out); break;
         case 4: int_probe_kernel<4><<<blocks, threads, 0, s>>>(iters, 0x00030003, 0x00050005, out); break;
         case 5: int_probe_kernel<5><<<blocks, threads, 0, s>>>(iters, 3, 5, out); break;
-        default: int_probe_kernel<6><<<blocks, threads, 0, s>>>(iters, 3, 5, out); break;
+        case 6: int_probe_kernel<6><<<blocks, threads, 0, s>>>(iters, 3, 5, out); break;
+        case 7: int_probe_kernel<7><<<blocks, threads, 0, s>>>(iters, 0x00030003, 0x00050005, out); break;
+        case 8: int_probe_kernel<8><<<blocks, threads, 0, s>>>(iters, 0x00030003, 0x00050005, out); break;
+        default: int_probe_kernel<9><<<blocks, threads, 0, s>>>(iters, 0x00030003, 0x00050005, out); break;
     }
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }

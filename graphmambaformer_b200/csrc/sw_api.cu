@@ -27,17 +27,10 @@ __host__ __device__ inline unsigned long long sw32_tb_words_api(int qlen, int W)
     return (unsigned long long)((last >> 3) + 1) * 32ull;
 }
 
-__host__ __device__ inline unsigned long long sw16_tb_words_api(int qlen, int W, int L) {
-    const long long V = 2 * L;
-    const long long P = (W + 2 > 4 * L) ? W + 2 : 4 * L;
-    const long long nstrips = (qlen + V - 1) / V;
-    const long long last = (nstrips - 1) * P + 2 * ((qlen - 1) % V) + W - 1;
-    return (unsigned long long)((last >> 2) + 1) * L;
-}
 
-// The int16x2 form is exact when no 16-bit value, sum or difference can wrap:
-// cells lie in [-(4*pmax + 2), smax] with smax = match * (min(qlen, tlen) + 1)
-// and pmax the largest penalty, and the traceback compares differences.
+// The biased 16x2 form is exact when no 16-bit value can wrap: biased cells
+// lie in [pmax, smax + 4*pmax + 2] with smax = match * (min(qlen, tlen) + 1)
+// and pmax the largest penalty; the traceback compares ordered differences.
 __host__ __device__ inline int max_penalty(int mism, int go, int ge) {
     const int m = mism > go ? mism : go;
     return m > ge ? m : ge;
@@ -45,7 +38,7 @@ __host__ __device__ inline int max_penalty(int mism, int go, int ge) {
 __host__ __device__ inline bool fits_int16(int qlen, int tlen, int match, int mism, int go, int ge) {
     const long long smax = (long long)match * ((qlen < tlen ? qlen : tlen) + 1);
     const int pmax = max_penalty(mism, go, ge);
-    return pmax <= 2048 && match <= 2048 && smax + 6LL * pmax + 64 <= 32767;
+    return pmax <= 2048 && match <= 2048 && smax + 6LL * pmax + 66 <= 65535;
 }
 
 __host__ __device__ inline int sw_class(int qlen, int tlen, int hb, int match, int mism, int go, int ge) {
@@ -129,7 +122,9 @@ static void fill_args(SwArgs& a, const gmf_pairs* pairs, const gmf_sw_params* pa
     a.gap_extend = params->gap_extend;
     a.x_drop = params->x_drop;
     a.max_hb = pairs->max_half_band;
-    a.neg16 = -(2 * max_penalty(params->mismatch_penalty, params->gap_open, params->gap_extend) + 2);
+    const int pmax = max_penalty(params->mismatch_penalty, params->gap_open, params->gap_extend);
+    a.zero16 = 4 * pmax + 2;
+    a.neg16 = 2 * pmax;
     a.score = res->score;
     a.q_end = res->query_end;
     a.t_end = res->target_end;
@@ -184,7 +179,7 @@ extern "C" size_t gmf_banded_sw_workspace_bytes(int32_t n_pairs, const int32_t* 
             if (with_traceback && ql > 0) {
                 // the larger of the int32 and int16x2 layouts, whichever class the pair gets
                 unsigned long long tb = sw32_tb_words_api(ql, W);
-                for (int L = 8; L <= 32; L <<= 1) tb = std::max(tb, sw16_tb_words_api(ql, W, L));
+                for (int L = 8; L <= 32; L <<= 1) tb = std::max(tb, sw16_tb_words_l(ql, W, L));
                 words += tb + (size_t)ql + tl + 1;
             }
         }
@@ -235,7 +230,7 @@ extern "C" int gmf_banded_sw(const gmf_pairs* pairs, const gmf_sw_params* params
     for (int c = 0; c < 3; ++c) {
         const int L = lanes[c];
         SwArgs ac = a;
-        ac.ring = ring_entries(std::max(0, cls_wmax[c] + 2 - 4 * L));
+        ac.ring = ring_entries(std::max(3, sw16_period(cls_wmax[c], L) - 4 * L - 1));
         const int wpb = warps_per_block((size_t)sw16_smem_per_warp(c, ac.ring), di);
         if (wpb == 0) return GMF_ERR_LIMIT;
         const int grid = di.sms * std::max(1, 16 / wpb);

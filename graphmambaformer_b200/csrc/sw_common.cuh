@@ -31,7 +31,8 @@ struct SwArgs {
     int32_t n_pairs;
     int32_t match, mismatch, gap_open, gap_extend, x_drop;
     int32_t max_hb;
-    int32_t neg16;                 // "-inf" of the int16x2 form: -(2 * max penalty + 2)
+    int32_t zero16;                // biased zero of the 16x2 form: 4 * max penalty + 2
+    int32_t neg16;                 // biased "-inf" of the 16x2 form: zero16 - (2 * max penalty + 2)
     int32_t ring;                  // delay-line entries per lane group (power of two)
     unsigned long long* counters;  // [0] workspace words handed out (bump allocator)
     int32_t* queue;                // [N_CLASSES] heads, [N_CLASSES] counts
@@ -51,6 +52,30 @@ struct SwArgs {
     unsigned long long* cigar_used;
     int32_t* err;
 };
+
+// Pipeline period of the 16x2 form: steps per strip of 2L rows, a multiple of
+// 4 so that rows start on 4-step chunk boundaries.
+__host__ __device__ inline int sw16_period(int W, int L) {
+    const int p = (W + 2 > 4 * L) ? W + 2 : 4 * L;
+    return (p + 3) & ~3;
+}
+
+// Traceback words of one pair in the 16x2 form (one word per lane per chunk).
+__host__ __device__ inline unsigned long long sw16_tb_words_l(int qlen, int W, int L) {
+    const long long V = 2 * L;
+    const long long P = sw16_period(W, L);
+    const long long nstrips = (qlen + V - 1) / V;
+    const long long last = (nstrips - 1) * P + 2 * ((qlen - 1) % V) + W - 1;
+    return (unsigned long long)((last >> 2) + 1) * L;
+}
+
+// PTX byte permute in the generic mode: selector nibbles with bit 3 set
+// replicate the sign of the selected byte.
+__device__ __forceinline__ unsigned prmt(unsigned a, unsigned b, unsigned sel) {
+    unsigned d;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(sel));
+    return d;
+}
 
 __device__ __forceinline__ int imax(int a, int b) { return a > b ? a : b; }
 __device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }

@@ -176,14 +176,16 @@ def test_rejects_band_beyond_limit(ext):
 
 
 def test_batched_and_plain_forms_agree_on_every_class(ext):
-    """int16x2 with 8/16/32 lanes, int32 (scores beyond int16), x-drop on and
-    off: the batched form equals the plain int32 form field for field."""
+    """16x2 cells with 8/16/32 lanes, int32 (scores beyond the 16-bit range),
+    x-drop on and off: the batched form equals the plain int32 form field for
+    field."""
     from graphmambaformer_b200 import synth
 
     rng = np.random.default_rng(21)
     ref = synth.random_reference(400_000, rng)
     qs, ts, hbs = [], [], []
-    for L, hb in ((80, 5), (300, 20), (900, 45), (600, 90), (2000, 200), (17_000, 40), (300, 0), (50, 300)):
+    for L, hb in ((80, 5), (300, 20), (900, 45), (600, 90), (2000, 200), (17_000, 40), (33_000, 30),
+                  (300, 0), (50, 300)):
         for _ in range(6):
             s = int(rng.integers(500, 350_000 - L))
             qs.append(synth.apply_errors(ref[s: s + L], synth.ONT, rng))
@@ -202,13 +204,14 @@ def test_batched_and_plain_forms_agree_on_every_class(ext):
 
 def test_int16_eligibility_boundary(ext):
     """Identical sequences whose scores sit just inside and just outside the
-    int16 range of the batched form (16-bit cells up to ~32.6k) agree with the
-    plain int32 form and with the closed-form score."""
+    16-bit range of the batched form (biased cells: score + 6*pmax + 66 <=
+    65535, i.e. up to 32,715 matching bases with these penalties) agree with
+    the plain int32 form and with the closed-form score."""
     from graphmambaformer_b200 import synth
 
     rng = np.random.default_rng(77)
     qs, ts = [], []
-    for n in (16_300, 16_330, 16_340, 16_400):
+    for n in (32_700, 32_715, 32_716, 32_800):
         s = synth.random_reference(n, rng)
         qs.append(s)
         ts.append(s.copy())
