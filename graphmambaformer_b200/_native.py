@@ -24,6 +24,7 @@ GMF_ERR_NOT_READY = 7
 
 GMF_SWF_WORKSPACE = 1
 GMF_SWF_CAPACITY = 2
+GMF_SWF_TIMEOUT = 4
 
 MAX_HALF_BAND = 4096
 MAX_READ_ANCHORS = 16384

@@ -36,6 +36,9 @@
 // chunk's first step in the top nibble), and checks the chunk's maxima for
 // the best cell (the first maximum in row-then-slot order is recovered from
 // the chunk's 4 kept H values when the maximum grows).
+//
+// Long pairs with wide bands run in the cooperative form below: the warps of
+// one CTA share a pair strip by strip.
 
 #include <algorithm>
 
@@ -77,6 +80,221 @@ __device__ __forceinline__ unsigned tsel(int u) {
     return u == 0 ? 0x4640u : (u == 1 ? 0x4041u : (u == 2 ? 0x4142u : 0x4243u));
 }
 
+// ---------------------------------------------------------------------------
+// Pieces shared by the one-warp and the cooperative (several warps per pair)
+// kernels.
+// ---------------------------------------------------------------------------
+
+// Per-lane DP state carried from step to step.
+struct Cells16 {
+    unsigned hv, fv, hd, ml, el;  // H / F of the row above (this and the previous slot), M / E on the left
+    unsigned ma, mb;              // slot - band_lo, band_hi - slot per half (negative = out of band)
+    unsigned qp;                  // query codes of the two rows (0x100 = never matches)
+    unsigned acc;                 // traceback nibbles of the chunk
+};
+
+// Scoring constants in packed biased form.
+struct K16 {
+    unsigned Z, NEGV, Z2, NEG2, GO2, GE2, MATCH2, NGE2, NZ2, MX;
+    __device__ explicit K16(const SwArgs& a) {
+        Z = (unsigned)a.zero16;
+        NEGV = (unsigned)a.neg16;
+        Z2 = Z * ONE2;
+        NEG2 = NEGV * ONE2;
+        GO2 = (unsigned)a.gap_open * ONE2;
+        GE2 = (unsigned)a.gap_extend * ONE2;
+        MATCH2 = (unsigned)a.match * ONE2;
+        NGE2 = ((0x10000u - (unsigned)a.gap_extend) & 0xFFFFu) * ONE2;  // -ext mod 2^16
+        NZ2 = ((0x10000u - Z) & 0xFFFFu) * ONE2;                        // -zero mod 2^16
+        MX = (unsigned)(a.match + a.mismatch);
+    }
+    __device__ unsigned init_pk() const { return Z | (NEGV << 16); }  // row 0: H = 0, F = -inf
+};
+
+__device__ __forceinline__ void cells_init(Cells16& c, const K16& K) {
+    c.hv = K.Z2;
+    c.fv = K.NEG2;
+    c.hd = K.Z2;
+    c.ml = K.NEG2;
+    c.el = K.NEG2;
+    c.ma = pack16(-30000, -30000);
+    c.mb = 0u;
+    c.qp = 0x01000100u;
+    c.acc = 0u;
+}
+
+// Target codes as 32-bit words of the whole target buffer, indexed from its
+// first aligned word; a chunk's 4 codes are a funnel shift of two words, and
+// the window slides one word per chunk with a load two chunks ahead.  Words
+// outside the buffer are clamped: they only ever feed out-of-band cells.
+struct TWin {
+    const uint32_t* w32;
+    int nwords;
+    long long pair_t;  // byte offset of the pair's codes from w32
+    unsigned w0, w1, w2;
+    int wi, tsh;
+    __device__ void setup(const SwArgs& a, const PairGeo& G, bool active) {
+        const long long tbase = (long long)(uintptr_t)a.t & ~3ll;
+        const long long t_total = active ? a.t_off[a.n_pairs] : 1;
+        const long long nw64 = (((long long)(uintptr_t)a.t + t_total - 1 - tbase) >> 2) + 1;
+        nwords = nw64 > 0x7fffffffll ? 0x7fffffff : (int)nw64;
+        w32 = reinterpret_cast<const uint32_t*>((uintptr_t)tbase);
+        pair_t = (long long)(uintptr_t)G.t - tbase;
+        w0 = w1 = w2 = 0u;
+        wi = 0;
+        tsh = 0;
+    }
+    __device__ unsigned ld(int i) const { return __ldg(w32 + imin(imax(i, 0), nwords - 1)); }
+    __device__ void start(int code_index, bool active) {  // window at code index `code_index` of the pair
+        const long long off = pair_t + (long long)code_index;
+        tsh = (int)(off & 3) * 8;
+        wi = (int)(off >> 2);
+        if (active) {
+            w0 = ld(wi);
+            w1 = ld(wi + 1);
+            w2 = ld(wi + 2);
+        }
+    }
+    __device__ unsigned window() const { return __funnelshift_r(w0, w1, tsh); }
+    __device__ void advance(bool active) {
+        w0 = w1;
+        w1 = w2;
+        ++wi;
+        if (active) w2 = ld(wi + 2);
+    }
+};
+
+// New rows for both halves of a lane: query codes and band intervals (the
+// high half's interval is expressed in the low half's slot, two steps later).
+__device__ __forceinline__ void row_start16(Cells16& c, int row, int j0, int qlen, int tlen, int W,
+                                            const int8_t* q) {
+    const int cq0 = row <= qlen ? (int)q[row - 1] : -1;
+    const int cq1 = row + 1 <= qlen ? (int)q[row] : -1;
+    c.qp = pack16((cq0 >= 0 && cq0 != 5) ? cq0 : 0x100, (cq1 >= 0 && cq1 != 5) ? cq1 : 0x100);
+    // interval bounds clamped into int16: an empty interval stays empty
+    const int lo0 = imin(imax(0, 1 - j0), 32000);
+    const int hi0 = row <= qlen ? imax(imin(W - 1, tlen - j0), -1) : -1;
+    const int lo1 = imin(imax(2, 2 - j0), 32000);
+    const int hi1 = row + 1 <= qlen ? imax(imin(W + 1, tlen - j0 + 1), -1) : -1;
+    c.ma = pack16(-1 - lo0, -1 - lo1);
+    c.mb = pack16(hi0 + 1, hi1 + 1);
+}
+
+// Four pipeline steps of one lane.  The first lane of the group takes its
+// row-above inputs from rv[] when `from_rv` (delay line or previous warp),
+// every other lane from lane k-1 by one shuffle of the packed (H.hi, F.hi).
+template <int L, bool TB, int EM>
+__device__ __forceinline__ void chunk16(Cells16& c, const K16& K, const Grp<L>& grp, int src, unsigned tw,
+                                        unsigned tpv, bool from_rv, const unsigned (&rv)[4],
+                                        unsigned (&hk)[4], unsigned (&pko)[4]) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const unsigned tp = prmt(tw, tpv, tsel(u));
+        const unsigned mis = flag2(c.qp ^ tp);  // 0: match, 1: mismatch
+        const unsigned diag = __vadd2(c.hd, __vsub2(K.MATCH2, mis * K.MX));
+        const unsigned fa = __vsub2(c.hv, K.GO2);
+        unsigned F = __viaddmax_u16x2(c.fv, K.NGE2, fa);  // max(F above - ext, H above - open)
+        unsigned M = __vimax3_u16x2(diag, F, K.Z2);
+        const unsigned ea = __vsub2(c.ml, K.GO2);
+        unsigned E = __viaddmax_u16x2(c.el, K.NGE2, ea);
+        unsigned H = umax2(M, E);
+        if (TB) {
+            const unsigned nz = __viaddmin_u16x2(H, K.NZ2, ONE2);  // H > 0
+            const unsigned n1 = flag2(__vsub2(H, diag));           // H != diag
+            const unsigned n2 = flag2(__vsub2(H, F));              // H != F
+            const unsigned fc = flag2(__vsub2(F, fa));             // F extends
+            unsigned ec = 0u;                                      // E extends
+            if (EM == 0) ec = flag2(__vsub2(E, ea));
+            if (EM == 2) ec = flag2(__vsub2(E, __vsub2(c.el, K.GE2))) ^ ONE2;
+            const unsigned b0 = nz & (~n1 | n2);  // diagonal or E, when H > 0
+            const unsigned b1 = nz & n1;          // F or E
+            const unsigned x = b0 + 2u * b1 + 4u * fc + 8u * ec;
+            c.acc = u == 0 ? x : c.acc * 16u + x;
+        }
+        // in-band mask: slot - lo >= 0 and hi - slot >= 0 per half
+        c.ma = __vadd2(c.ma, ONE2);
+        c.mb = __vsub2(c.mb, ONE2);
+        const unsigned m = prmt(c.ma | c.mb, 0u, 0xBB99u);  // 0xFFFF per out-of-band half
+        H = (H & ~m) | (K.Z2 & m);
+        F = (F & ~m) | (K.NEG2 & m);
+        M = (M & ~m) | (K.NEG2 & m);
+        E = (E & ~m) | (K.NEG2 & m);
+        const unsigned pk = prmt(H, F, 0x7632u);  // (H.hi, F.hi)
+        unsigned sh = grp.shfl(pk, src);
+        if (from_rv) sh = rv[u];
+        c.hd = c.hv;
+        c.hv = prmt(sh, H, 0x5410u);  // low: row above (lane k-1 high), high: own low
+        c.fv = prmt(sh, F, 0x5432u);
+        c.ml = M;
+        c.el = E;
+        hk[u] = H;
+        pko[u] = pk;
+    }
+}
+
+// Best-cell bookkeeping of a chunk: `lb` is the running maximum per half (the
+// row maximum under x-drop); when it grows, the first of the chunk's 4 steps
+// that reaches it gives the position (global step, or slot under x-drop).
+template <bool XD>
+__device__ __forceinline__ void best16(unsigned& lb, int& pos0, int& pos1, const unsigned (&hk)[4], int gstep,
+                                       int d) {
+    const unsigned cm = umax2(umax2(hk[0], hk[1]), umax2(hk[2], hk[3]));
+    const unsigned nb = umax2(lb, cm);
+    if (nb != lb) {
+        const unsigned inc = nb ^ lb;
+        if (inc & 0xFFFFu) {
+            const int t = lo16(nb);
+            const int u = lo16(hk[0]) == t ? 0 : (lo16(hk[1]) == t ? 1 : (lo16(hk[2]) == t ? 2 : 3));
+            pos0 = XD ? d + u : gstep + u;
+        }
+        if (inc >> 16) {
+            const int t = hi16(nb);
+            const int u = hi16(hk[0]) == t ? 0 : (hi16(hk[1]) == t ? 1 : (hi16(hk[2]) == t ? 2 : 3));
+            pos1 = XD ? d + u - 2 : gstep + u;
+        }
+        lb = nb;
+    }
+}
+
+// Best cell of a lane (non-x-drop): the first maximum of each half, from its
+// global step, as (score, row, slot).
+template <int L>
+__device__ __forceinline__ void lane_best16(unsigned lb, int pos0, int pos1, unsigned Z, int k, int P,
+                                            int& bh, int& bi, int& bd) {
+    constexpr int V = 2 * L;
+    const int v0 = lo16(lb) - (int)Z, v1 = hi16(lb) - (int)Z;
+    int r0 = 0, s0 = 0, r1 = 0, s1 = 0;
+    if (v0 > 0) {
+        const int tt = pos0 - 2 * (2 * k);
+        const int s = tt / P;
+        r0 = s * V + 2 * k + 1;
+        s0 = tt - s * P;
+    }
+    if (v1 > 0) {
+        const int tt = pos1 - 2 * (2 * k + 1);
+        const int s = tt / P;
+        r1 = s * V + 2 * k + 2;
+        s1 = tt - s * P;
+    }
+    bh = v0;
+    bi = r0;
+    bd = s0;
+    if (v1 > bh || (v1 == bh && v1 > 0 && (r1 < bi || (r1 == bi && s1 < bd)))) {
+        bh = v1;
+        bi = r1;
+        bd = s1;
+    }
+}
+
+// (score, row, slot) ordering of the best cell: higher score, then earlier
+// row, then earlier slot.
+__device__ __forceinline__ bool better_cell(int oh, int oi, int od, int bh, int bi, int bd) {
+    return oh > bh || (oh == bh && (oi < bi || (oi == bi && od < bd)));
+}
+
+// ---------------------------------------------------------------------------
+// One group of L lanes per pair.
+// ---------------------------------------------------------------------------
 template <int L, bool TB, bool XD, int EM>
 __device__ void sw16_group(const SwArgs& a, int p, const Grp<L>& grp, uint32_t* ring) {
     constexpr int V = 2 * L;
@@ -106,158 +324,58 @@ __device__ void sw16_group(const SwArgs& a, int p, const Grp<L>& grp, uint32_t* 
     const int loop_last = __reduce_max_sync(FULL_MASK, my_last);
     const int last_chunk = my_last >> 2;  // -1 when inactive
 
-    const unsigned Z = (unsigned)a.zero16, NEGV = (unsigned)a.neg16;
-    const unsigned Z2 = Z * ONE2, NEG2 = NEGV * ONE2;
-    const unsigned GO2 = (unsigned)a.gap_open * ONE2;
-    const unsigned GE2 = (unsigned)a.gap_extend * ONE2;
-    const unsigned MATCH2 = (unsigned)a.match * ONE2;
-    const unsigned NGE2 = ((0x10000u - (unsigned)a.gap_extend) & 0xFFFFu) * ONE2;  // -ext mod 2^16
-    const unsigned NZ2 = ((0x10000u - Z) & 0xFFFFu) * ONE2;                        // -zero mod 2^16
-    const unsigned MX = (unsigned)(a.match + a.mismatch);
-    for (int x = k; x < a.ring; x += L) ring[x] = Z | (NEGV << 16);  // row 0: H = 0, F = -inf
+    const K16 K(a);
+    for (int x = k; x < a.ring; x += L) ring[x] = K.init_pk();
     __syncwarp();
-
-    // target codes: 32-bit words of the whole target buffer, indexed from its
-    // first aligned word; the window of a chunk is a funnel shift of two words
-    const long long tbase = (long long)(uintptr_t)a.t & ~3ll;
-    const long long t_total = active ? a.t_off[a.n_pairs] : 1;  // codes in the buffer
-    const long long tend = (long long)(uintptr_t)a.t + t_total;  // one past the last code
-    const long long nw64 = ((tend - 1 - tbase) >> 2) + 1;
-    const int nwords = nw64 > 0x7fffffffll ? 0x7fffffff : (int)nw64;
-    const uint32_t* tw32 = reinterpret_cast<const uint32_t*>((uintptr_t)tbase);
-    const long long pair_t = (long long)(uintptr_t)G.t - tbase;  // byte offset of the pair's codes
+    TWin tw;
+    tw.setup(a, G, active);
 
     const int8_t* __restrict__ q = G.q;
     const int c0 = G.off - G.hb;  // j = row + c0 + d
     int d = -4 * k;               // slot of the low half at the chunk start
     int row = 2 * k + 1 - V;      // row of the low half (advanced by V at each row start)
-    unsigned ma = pack16(-30000, -30000), mb = 0u;  // slot - band_lo, band_hi - slot (per half)
-    unsigned qp = 0x01000100u;
-    unsigned hv = Z2, fv = NEG2, hd = Z2, ml = NEG2, el = NEG2;
-    unsigned w0 = 0u, w1 = 0u, w2 = 0u, tpv = 0u;
-    int wi = 0, tsh = 0;
-    unsigned acc = 0u;
-    unsigned lb = Z2;  // best H so far per half (non-x-drop) / row max (x-drop)
+    Cells16 c;
+    cells_init(c, K);
+    unsigned tpv = 0u;
+    unsigned lb = K.Z2;  // best H so far per half (non-x-drop) / row max (x-drop)
     int pos0 = 0, pos1 = 0;
-    unsigned rv0 = 0u, rv1 = 0u, rv2 = 0u, rv3 = 0u;  // delay-line entries of the chunk
+    unsigned rv[4] = {0u, 0u, 0u, 0u};  // delay-line entries of the chunk
     const int src = (k + L - 1) & (L - 1);
+    const bool from_rv = use_ring && k == 0;
     const int dW0 = (W - 1) & ~3, dW1 = (W + 1) & ~3;  // chunks that end a row (x-drop)
 
     for (int g0 = 0; g0 <= loop_last; g0 += 4) {
         if (d == 0) {  // both halves start new rows (the high half two steps later)
             row += V;
-            const int j0 = row + c0;
-            const int cq0 = row <= qlen ? (int)q[row - 1] : -1;
-            const int cq1 = row + 1 <= qlen ? (int)q[row] : -1;
-            qp = pack16((cq0 >= 0 && cq0 != 5) ? cq0 : 0x100, (cq1 >= 0 && cq1 != 5) ? cq1 : 0x100);
-            // interval bounds clamped into int16: an empty interval stays empty
-            const int lo0 = imin(imax(0, 1 - j0), 32000);
-            const int hi0 = row <= qlen ? imax(imin(W - 1, tlen - j0), -1) : -1;
-            const int lo1 = imin(imax(2, 2 - j0), 32000);
-            const int hi1 = row + 1 <= qlen ? imax(imin(W + 1, tlen - j0 + 1), -1) : -1;
-            ma = pack16(-1 - lo0, -1 - lo1);
-            mb = pack16(hi0 + 1, hi1 + 1);
-            // target window at code index j0 - 1 of the pair (words outside the
-            // buffer are clamped: they only feed out-of-band cells)
-            const long long off = pair_t + (long long)(j0 - 1);
-            tsh = (int)(off & 3) * 8;
-            wi = (int)(off >> 2);
-            if (active) {
-                w0 = __ldg(tw32 + imin(imax(wi, 0), nwords - 1));
-                w1 = __ldg(tw32 + imin(imax(wi + 1, 0), nwords - 1));
-                w2 = __ldg(tw32 + imin(imax(wi + 2, 0), nwords - 1));
-            }
+            row_start16(c, row, row + c0, qlen, tlen, W, q);
+            tw.start(row + c0 - 1, active);
             tpv = 0u;
             if (XD) {
-                lb = Z2;
+                lb = K.Z2;
                 pos0 = 0;
                 pos1 = 0;
             }
         }
-        if (use_ring && k == 0) {
+        if (from_rv) {
             const uint4 r = *reinterpret_cast<const uint4*>(ring + ((g0 - D) & rmask));
-            rv0 = r.x;
-            rv1 = r.y;
-            rv2 = r.z;
-            rv3 = r.w;
+            rv[0] = r.x;
+            rv[1] = r.y;
+            rv[2] = r.z;
+            rv[3] = r.w;
         }
-        const unsigned tw = __funnelshift_r(w0, w1, tsh);
-        unsigned hk0, hk1, hk2, hk3, pk0, pk1, pk2, pk3;
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const unsigned tp = prmt(tw, tpv, tsel(u));
-            const unsigned mis = flag2(qp ^ tp);  // 0: match, 1: mismatch
-            const unsigned diag = __vadd2(hd, __vsub2(MATCH2, mis * MX));
-            const unsigned fa = __vsub2(hv, GO2);
-            unsigned F = __viaddmax_u16x2(fv, NGE2, fa);  // max(F above - ext, H above - open)
-            unsigned M = __vimax3_u16x2(diag, F, Z2);
-            const unsigned ea = __vsub2(ml, GO2);
-            unsigned E = __viaddmax_u16x2(el, NGE2, ea);
-            unsigned H = umax2(M, E);
-            if (TB) {
-                const unsigned nz = __viaddmin_u16x2(H, NZ2, ONE2);  // H > 0
-                const unsigned n1 = flag2(__vsub2(H, diag));         // H != diag
-                const unsigned n2 = flag2(__vsub2(H, F));            // H != F
-                const unsigned fc = flag2(__vsub2(F, fa));           // F extends
-                unsigned ec = 0u;                                    // E extends
-                if (EM == 0) ec = flag2(__vsub2(E, ea));
-                if (EM == 2) ec = flag2(__vsub2(E, __vsub2(el, GE2))) ^ ONE2;
-                const unsigned b0 = nz & (~n1 | n2);  // diagonal or E, when H > 0
-                const unsigned b1 = nz & n1;          // F or E
-                const unsigned x = b0 + 2u * b1 + 4u * fc + 8u * ec;
-                acc = u == 0 ? x : acc * 16u + x;
-            }
-            // in-band mask: slot - lo >= 0 and hi - slot >= 0 per half
-            ma = __vadd2(ma, ONE2);
-            mb = __vsub2(mb, ONE2);
-            const unsigned m = prmt(ma | mb, 0u, 0xBB99u);  // 0xFFFF per out-of-band half
-            H = (H & ~m) | (Z2 & m);
-            F = (F & ~m) | (NEG2 & m);
-            M = (M & ~m) | (NEG2 & m);
-            E = (E & ~m) | (NEG2 & m);
-            const unsigned pk = prmt(H, F, 0x7632u);  // (H.hi, F.hi)
-            unsigned sh = grp.shfl(pk, src);
-            if (use_ring && k == 0) sh = u == 0 ? rv0 : (u == 1 ? rv1 : (u == 2 ? rv2 : rv3));
-            hd = hv;
-            hv = prmt(sh, H, 0x5410u);  // low: row above (lane k-1 high), high: own low
-            fv = prmt(sh, F, 0x5432u);
-            ml = M;
-            el = E;
-            if (u == 0) { hk0 = H; pk0 = pk; }
-            if (u == 1) { hk1 = H; pk1 = pk; }
-            if (u == 2) { hk2 = H; pk2 = pk; }
-            if (u == 3) { hk3 = H; pk3 = pk; }
-        }
+        const unsigned twin = tw.window();
+        unsigned hk[4], pk[4];
+        chunk16<L, TB, EM>(c, K, grp, src, twin, tpv, from_rv, rv, hk, pk);
         // ---- once per chunk ----
-        tpv = prmt(tw, tpv, 0x4344u);  // this chunk's last code, for the next chunk's high half
-        w0 = w1;
-        w1 = w2;
-        ++wi;
-        if (active) w2 = __ldg(tw32 + imin(imax(wi + 2, 0), nwords - 1));
-        if (TB && (g0 >> 2) <= last_chunk) bits[(g0 >> 2) * L + k] = acc;
+        tpv = prmt(twin, tpv, 0x4344u);  // this chunk's last code, for the next chunk's high half
+        tw.advance(active);
+        if (TB && (g0 >> 2) <= last_chunk) bits[(g0 >> 2) * L + k] = c.acc;
         if (use_ring && k == L - 1)
-            *reinterpret_cast<uint4*>(ring + (g0 & rmask)) = make_uint4(pk0, pk1, pk2, pk3);
-        {
-            const unsigned cm = umax2(umax2(hk0, hk1), umax2(hk2, hk3));
-            const unsigned nb = umax2(lb, cm);
-            if (nb != lb) {  // the maximum grew in this chunk: first step reaching it
-                const unsigned inc = nb ^ lb;
-                if (inc & 0xFFFFu) {
-                    const int t = lo16(nb);
-                    const int u = lo16(hk0) == t ? 0 : (lo16(hk1) == t ? 1 : (lo16(hk2) == t ? 2 : 3));
-                    pos0 = XD ? d + u : g0 + u;
-                }
-                if (inc >> 16) {
-                    const int t = hi16(nb);
-                    const int u = hi16(hk0) == t ? 0 : (hi16(hk1) == t ? 1 : (hi16(hk2) == t ? 2 : 3));
-                    pos1 = XD ? d + u - 2 : g0 + u;
-                }
-                lb = nb;
-            }
-            if (XD) {
-                if (d == dW0 && row <= qlen && row >= 1) rowmax[row - 1] = make_int2(lo16(lb) - (int)Z, pos0);
-                if (d == dW1 && row + 1 <= qlen && row >= 1) rowmax[row] = make_int2(hi16(lb) - (int)Z, pos1);
-            }
+            *reinterpret_cast<uint4*>(ring + (g0 & rmask)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        best16<XD>(lb, pos0, pos1, hk, g0, d);
+        if (XD) {
+            if (d == dW0 && row <= qlen && row >= 1) rowmax[row - 1] = make_int2(lo16(lb) - (int)K.Z, pos0);
+            if (d == dW1 && row + 1 <= qlen && row >= 1) rowmax[row] = make_int2(hi16(lb) - (int)K.Z, pos1);
         }
         __syncwarp();
         d += 4;
@@ -269,35 +387,13 @@ __device__ void sw16_group(const SwArgs& a, int p, const Grp<L>& grp, uint32_t* 
     if (XD) {
         xdrop_best<L>(grp, rowmax, qlen, a.x_drop, active, bh, bi, bd);
     } else {
-        // first cell of each virtual lane's maximum, then the group's best
-        const int v0 = lo16(lb) - (int)Z, v1 = hi16(lb) - (int)Z;
-        int r0 = 0, s0 = 0, r1 = 0, s1 = 0;
-        if (v0 > 0) {
-            const int tt = pos0 - 2 * (2 * k);
-            const int s = tt / P;
-            r0 = s * V + 2 * k + 1;
-            s0 = tt - s * P;
-        }
-        if (v1 > 0) {
-            const int tt = pos1 - 2 * (2 * k + 1);
-            const int s = tt / P;
-            r1 = s * V + 2 * k + 2;
-            s1 = tt - s * P;
-        }
-        bh = v0;
-        bi = r0;
-        bd = s0;
-        if (v1 > bh || (v1 == bh && v1 > 0 && (r1 < bi || (r1 == bi && s1 < bd)))) {
-            bh = v1;
-            bi = r1;
-            bd = s1;
-        }
+        lane_best16<L>(lb, pos0, pos1, K.Z, k, P, bh, bi, bd);
 #pragma unroll
         for (int o = L / 2; o > 0; o >>= 1) {
             const int oh = grp.xr(bh, o);
             const int oi = grp.xr(bi, o);
             const int od = grp.xr(bd, o);
-            if (oh > bh || (oh == bh && (oi < bi || (oi == bi && od < bd)))) {
+            if (better_cell(oh, oi, od, bh, bi, bd)) {
                 bh = oh;
                 bi = oi;
                 bd = od;
@@ -347,6 +443,261 @@ __global__ void __launch_bounds__(128) sw16_kernel(SwArgs a) {
         const int p = idx < count ? list[idx] : -1;
         sw16_group<L, TB, XD, EM>(a, p, grp, ring);
     }
+}
+
+// ---------------------------------------------------------------------------
+// Cooperative form: the NW warps of one CTA align one long pair.
+//
+// Warp w runs strips w, w+NW, w+2NW, ... of the pair with the one-warp
+// pipeline; the first lane of each strip reads the row above (the last lane's
+// (H.hi, F.hi) of the strip before) from the previous warp's shared-memory
+// ring instead of its own delay line.  Entry e of warp w's ring is its last
+// lane's output at warp-local step e; warp w reads entry t + 4L of warp w-1
+// at its local step t (t + 4L - P from warp NW-1 for warp 0), so each warp
+// runs at least 4L + 4 steps behind its predecessor, and the cycle of NW
+// warps keeps moving only when P >= NW * (4L + 4) -- the classifier sends a
+// pair here only then.  Under that bound no writer is ever more than P
+// entries ahead of its reader, so a ring of R >= P + 8 entries needs no
+// back-pressure.  Each writer publishes its progress after every chunk (ring
+// store, block fence, flag store); each reader spins on the flag with an
+// iteration limit, after which it records GMF_SWF_TIMEOUT and goes on.
+// Traceback words land at the same (global step, lane) positions as in the
+// one-warp layout, so the walk (warp 0, after a block barrier) is unchanged.
+// ---------------------------------------------------------------------------
+constexpr int COOP_WAIT_LIMIT = 1 << 22;  // spins (about 20 ns each) before a wait gives up
+
+template <int NW, bool TB, bool XD, int EM>
+__device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, volatile int* prog, int (*sbest)[3],
+                               uint32_t** sws) {
+    constexpr int L = 32, V = 64;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    Grp<32> grp(lane);
+    PairGeo G = load_geo(a, p);
+    const bool bad = G.hb < 0 || G.hb > a.max_hb;
+    if (bad || G.qlen <= 0 || G.tlen <= 0) {  // uniform over the CTA
+        if (threadIdx.x == 0) write_empty<TB>(a, p, bad);
+        return;
+    }
+    const int qlen = G.qlen, tlen = G.tlen, W = G.W;
+    const int P = sw16_period(W, L);
+    G.P = P;
+    const int nstrips = (qlen + V - 1) / V;
+    const int my_last = (nstrips - 1) * P + 2 * ((qlen - 1) % V) + W - 1;  // global step of the last cell
+    const int last_chunk = my_last >> 2;
+
+    const unsigned long long tbw = TB ? sw16_tb_words_l(qlen, W, L) : 0ull;
+    if (w == 0) {
+        uint32_t* ws0 = ws_alloc<32>(a, grp, tbw + (XD ? 2ull * qlen : 0ull), TB || XD);
+        if (lane == 0) *sws = ws0;
+    }
+    if (threadIdx.x < NW) prog[threadIdx.x] = 0;
+    __syncthreads();
+    uint32_t* ws = *sws;
+    if ((TB || XD) && !ws) {
+        if (threadIdx.x == 0) write_empty<TB>(a, p, true);
+        return;
+    }
+    uint32_t* bits = ws;
+    int2* rowmax = XD ? reinterpret_cast<int2*>(ws + tbw) : nullptr;
+
+    const K16 K(a);
+    TWin tw;
+    tw.setup(a, G, true);
+    const int8_t* __restrict__ q = G.q;
+    const int c0 = G.off - G.hb;
+    const int kk_last = w < nstrips ? (nstrips - 1 - w) / NW : -1;  // this warp's last strip (local index)
+    const int loop_end = (kk_last + 1) * P + 4 * L + 4;             // drains what the next warp may read
+    uint32_t* ring_out = rings + (size_t)w * a.ring;
+    const int wprev = (w + NW - 1) % NW;
+    const uint32_t* ring_in = rings + (size_t)wprev * a.ring;
+    const int rmask = a.ring - 1;
+    const unsigned INIT = K.init_pk();
+
+    int d = -4 * lane;  // slot of the low half at the chunk start
+    int kk = -1;        // local index of the lane's current strip
+    int row = 0, gofs = 0;
+    Cells16 c;
+    cells_init(c, K);
+    unsigned tpv = 0u, lb = K.Z2;
+    int pos0 = 0, pos1 = 0;
+    unsigned rv[4] = {INIT, INIT, INIT, INIT};
+    const int src = (lane + 31) & 31;
+    const int dW0 = (W - 1) & ~3, dW1 = (W + 1) & ~3;
+
+    if (kk_last >= 0) {
+        for (int t = 0; t < loop_end; t += 4) {
+            if (d == 0) {
+                ++kk;
+                const int s = w + NW * kk;
+                row = s * V + 2 * lane + 1;
+                gofs = (s - kk) * P;  // local step -> step of the one-warp schedule
+                row_start16(c, row, row + c0, qlen, tlen, W, q);
+                tw.start(row + c0 - 1, true);
+                tpv = 0u;
+                if (XD) {
+                    lb = K.Z2;
+                    pos0 = 0;
+                    pos1 = 0;
+                }
+            }
+            if (lane == 0) {
+                const int s0 = w + NW * kk;  // lane 0 starts its strips at t = kk * P
+                if (s0 >= 1 && s0 < nstrips) {
+                    const int e = t + 4 * L - (w == 0 ? P : 0);
+                    int spins = 0;
+                    while (prog[wprev] < e + 4) {
+                        // bounded: after the limit, or once any wait in the grid gave up
+                        // (every later wait then ends within ~1k spins), record and go on
+                        if (++spins > COOP_WAIT_LIMIT ||
+                            ((spins & 1023) == 0 && (*(volatile int*)a.err & (int)GMF_SWF_TIMEOUT))) {
+                            atomicOr(a.err, (int)GMF_SWF_TIMEOUT);
+                            break;
+                        }
+                        __nanosleep(20);
+                    }
+                    __threadfence_block();
+                    const uint4 r = *reinterpret_cast<const uint4*>(ring_in + (e & rmask));
+                    rv[0] = r.x;
+                    rv[1] = r.y;
+                    rv[2] = r.z;
+                    rv[3] = r.w;
+                } else {
+                    rv[0] = rv[1] = rv[2] = rv[3] = INIT;  // row 0, or a strip past the query
+                }
+            }
+            const unsigned twin = tw.window();
+            unsigned hk[4], pk[4];
+            chunk16<32, TB, EM>(c, K, grp, src, twin, tpv, lane == 0, rv, hk, pk);
+            tpv = prmt(twin, tpv, 0x4344u);
+            tw.advance(true);
+            const int g0 = t + gofs;
+            if (TB && kk >= 0 && (g0 >> 2) <= last_chunk) bits[(g0 >> 2) * L + lane] = c.acc;
+            if (lane == 31) {
+                *reinterpret_cast<uint4*>(ring_out + (t & rmask)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                __threadfence_block();
+                prog[w] = t + 4;
+            }
+            best16<XD>(lb, pos0, pos1, hk, g0, d);
+            if (XD && kk >= 0) {
+                if (d == dW0 && row <= qlen) rowmax[row - 1] = make_int2(lo16(lb) - (int)K.Z, pos0);
+                if (d == dW1 && row + 1 <= qlen) rowmax[row] = make_int2(hi16(lb) - (int)K.Z, pos1);
+            }
+            __syncwarp();
+            d += 4;
+            if (d == P) d = 0;
+        }
+    }
+    __syncthreads();  // every traceback word and row maximum is written
+
+    int bh = 0, bi = 0, bd = 0;
+    if (!XD) {
+        lane_best16<L>(lb, pos0, pos1, K.Z, lane, P, bh, bi, bd);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const int oh = grp.xr(bh, o);
+            const int oi = grp.xr(bi, o);
+            const int od = grp.xr(bd, o);
+            if (better_cell(oh, oi, od, bh, bi, bd)) {
+                bh = oh;
+                bi = oi;
+                bd = od;
+            }
+        }
+        if (lane == 0) {
+            sbest[w][0] = bh;
+            sbest[w][1] = bi;
+            sbest[w][2] = bd;
+        }
+        __syncthreads();
+    }
+    if (w != 0) return;
+    if (XD) {
+        xdrop_best<L>(grp, rowmax, qlen, a.x_drop, true, bh, bi, bd);
+    } else {
+        bh = sbest[0][0];
+        bi = sbest[0][1];
+        bd = sbest[0][2];
+        for (int x = 1; x < NW; ++x)
+            if (better_cell(sbest[x][0], sbest[x][1], sbest[x][2], bh, bi, bd)) {
+                bh = sbest[x][0];
+                bi = sbest[x][1];
+                bd = sbest[x][2];
+            }
+    }
+    const int qe = bh > 0 ? bi : 0;
+    const int te = bh > 0 ? bi + G.off - G.hb + bd : 0;
+    if (lane == 0) {
+        a.score[p] = bh;
+        a.q_end[p] = qe;
+        a.t_end[p] = te;
+    }
+    if (!TB) return;
+    RunWriter rw;
+    uint32_t* runs = ws_alloc<32>(a, grp, (unsigned long long)qe + te + 1, bh > 0);
+    const bool runs_ok = bh == 0 || runs != nullptr;
+    if (!runs_ok && lane == 0) atomicOr(a.err, (int)GMF_SWF_WORKSPACE);
+    rw.init(runs);
+    Layout16<L> lay{bits, P, W, qlen};
+    int qs = 0, ts = 0;
+    walk<L>(grp, lay, G, qe, te, runs_ok && bh > 0, rw, qs, ts);
+    finish_cigar<L>(a, grp, p, true, rw, runs_ok, qs, ts);
+}
+
+template <int NW, bool TB, bool XD, int EM>
+__global__ void __launch_bounds__(32 * NW) sw16_coop_kernel(SwArgs a) {
+    extern __shared__ uint4 coop_ring4[];
+    uint32_t* rings = reinterpret_cast<uint32_t*>(coop_ring4);
+    __shared__ volatile int prog[NW];
+    __shared__ int sbest[NW][3];
+    __shared__ uint32_t* sws;
+    __shared__ int spair;
+    constexpr int CLS = NW == 2 ? CLS_I16_C2 : (NW == 4 ? CLS_I16_C4 : CLS_I16_C8);
+    const int count = a.queue[N_CLASSES + CLS];
+    const int32_t* list = a.lists + (size_t)CLS * a.n_pairs;
+    for (;;) {
+        if (threadIdx.x == 0) spair = atomicAdd(&a.queue[CLS], 1);
+        __syncthreads();
+        const int idx = spair;
+        if (idx >= count) break;
+        sw16_coop_pair<NW, TB, XD, EM>(a, list[idx], rings, prog, sbest, &sws);
+        __syncthreads();
+    }
+}
+
+int sw16_coop_warps(int cls) { return cls == CLS_I16_C2 ? 2 : (cls == CLS_I16_C4 ? 4 : 8); }
+
+template <int NW, bool TB, bool XD, int EM>
+static int launch_coop(const SwArgs& a, cudaStream_t stream) {
+    const size_t smem = (size_t)NW * a.ring * sizeof(uint32_t);
+    void (*k)(SwArgs) = sw16_coop_kernel<NW, TB, XD, EM>;
+    if (smem > 48 * 1024)
+        GMF_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int dev = 0, sms = 0, per_sm = 0;
+    GMF_CUDA_TRY(cudaGetDevice(&dev));
+    GMF_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    GMF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * NW, smem));
+    if (per_sm <= 0) return GMF_ERR_LIMIT;
+    k<<<sms * per_sm, 32 * NW, smem, stream>>>(a);
+    return cuda_status(cudaGetLastError());
+}
+
+template <int NW, bool TB, bool XD>
+static int launch_coop_e(const SwArgs& a, int e_mode, cudaStream_t s) {
+    if (e_mode == 0) return launch_coop<NW, TB, XD, 0>(a, s);
+    if (e_mode == 1) return launch_coop<NW, TB, XD, 1>(a, s);
+    return launch_coop<NW, TB, XD, 2>(a, s);
+}
+
+template <int NW>
+static int launch_coop_x(const SwArgs& a, bool tb, bool xd, int e_mode, cudaStream_t s) {
+    if (tb) return xd ? launch_coop_e<NW, true, true>(a, e_mode, s) : launch_coop_e<NW, true, false>(a, e_mode, s);
+    return xd ? launch_coop_e<NW, false, true>(a, e_mode, s) : launch_coop_e<NW, false, false>(a, e_mode, s);
+}
+
+int launch_sw16_coop(const SwArgs& a, int cls, bool tb, bool xd, int e_mode, cudaStream_t stream) {
+    if (cls == CLS_I16_C2) return launch_coop_x<2>(a, tb, xd, e_mode, stream);
+    if (cls == CLS_I16_C4) return launch_coop_x<4>(a, tb, xd, e_mode, stream);
+    return launch_coop_x<8>(a, tb, xd, e_mode, stream);
 }
 
 int sw16_smem_per_warp(int cls, int ring) {

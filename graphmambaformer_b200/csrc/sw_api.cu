@@ -41,11 +41,23 @@ __host__ __device__ inline bool fits_int16(int qlen, int tlen, int match, int mi
     return pmax <= 2048 && match <= 2048 && smax + 6LL * pmax + 66 <= 65535;
 }
 
+// Class of a pair.  Narrow bands share a warp (8 or 16 lanes per pair); wide
+// bands get a warp; long pairs with wide bands get 2, 4 or 8 warps of one CTA
+// when their period lets that many warps run concurrently (P >= NW * (4*32 +
+// 4)) and the pair has at least two strips per warp.  Each cooperative class
+// covers one period range [NW * 132, 2 * NW * 132) (the 8-warp class up to
+// COOP_PMAX); shorter pairs in those ranges take one warp.
 __host__ __device__ inline int sw_class(int qlen, int tlen, int hb, int match, int mism, int go, int ge) {
     if (!fits_int16(qlen, tlen, match, mism, go, ge)) return CLS_I32;
     const int W = 2 * hb + 1;
     if (W <= 61) return CLS_I16_L8;
     if (W <= 125) return CLS_I16_L16;
+    const int P = sw16_period(W, 32);
+    const int strips = (qlen + 63) / 64;
+    // each cooperative class holds one period range (its rings are sized for it)
+    if (P >= 8 * 132 && P <= COOP_PMAX) return strips >= 16 ? CLS_I16_C8 : CLS_I16_L32;
+    if (P >= 4 * 132 && P < 8 * 132) return strips >= 8 ? CLS_I16_C4 : CLS_I16_L32;
+    if (P >= 2 * 132 && P < 4 * 132) return strips >= 4 ? CLS_I16_C2 : CLS_I16_L32;
     return CLS_I16_L32;
 }
 
@@ -224,7 +236,20 @@ extern "C" int gmf_banded_sw(const gmf_pairs* pairs, const gmf_sw_params* params
     GMF_CUDA_TRY(cudaGetLastError());
 
     const int Wmax = 2 * pairs->max_half_band + 1;
-    // int16x2 classes (a class only ever holds pairs up to its own band limit)
+    // cooperative classes first (the longest pairs), each with a ring of
+    // P + 8 entries per warp for the largest period the class can hold
+    const int Pmax = sw16_period(Wmax, 32);
+    const int coop_cls[3] = {CLS_I16_C8, CLS_I16_C4, CLS_I16_C2};
+    const int coop_pmin[3] = {8 * 132, 4 * 132, 2 * 132};
+    const int coop_pcap[3] = {COOP_PMAX, 8 * 132 - 4, 4 * 132 - 4};
+    for (int c = 0; c < 3; ++c) {
+        if (Pmax < coop_pmin[c]) continue;  // no pair can be in this class
+        SwArgs ac = a;
+        ac.ring = ring_entries(std::min(Pmax, coop_pcap[c]) + 7);
+        if ((size_t)sw16_coop_warps(coop_cls[c]) * ac.ring * 4 > (size_t)di.smem_optin) return GMF_ERR_LIMIT;
+        GMF_TRY(launch_sw16_coop(ac, coop_cls[c], tb, xd, em, stream));
+    }
+    // one-warp and shared-warp classes (a class only ever holds pairs up to its own band limit)
     const int cls_wmax[3] = {std::min(Wmax, 61), std::min(Wmax, 125), Wmax};
     const int lanes[3] = {8, 16, 32};
     for (int c = 0; c < 3; ++c) {

@@ -13,11 +13,14 @@ namespace gmf {
 
 // Pair classes of the batched form (device-side classifier).
 enum SwClass : int {
-    CLS_I16_L8 = 0,   // int16x2, 8 lanes per pair (W <= 61)
-    CLS_I16_L16 = 1,  // int16x2, 16 lanes per pair (W <= 125)
-    CLS_I16_L32 = 2,  // int16x2, 32 lanes per pair
-    CLS_I32 = 3,      // int32, 32 lanes per pair (scores beyond int16)
-    N_CLASSES = 4
+    CLS_I16_L8 = 0,   // 16x2, 8 lanes per pair (W <= 61)
+    CLS_I16_L16 = 1,  // 16x2, 16 lanes per pair (W <= 125)
+    CLS_I16_L32 = 2,  // 16x2, 32 lanes per pair
+    CLS_I32 = 3,      // int32, 32 lanes per pair (scores beyond the 16-bit range)
+    CLS_I16_C2 = 4,   // 16x2, 2 warps of one CTA per pair (264 <= P < 528)
+    CLS_I16_C4 = 5,   // 16x2, 4 warps of one CTA per pair (528 <= P < 1056)
+    CLS_I16_C8 = 6,   // 16x2, 8 warps of one CTA per pair (1056 <= P <= COOP_PMAX)
+    N_CLASSES = 7
 };
 
 struct SwArgs {
@@ -377,6 +380,10 @@ __device__ void finish_cigar(const SwArgs& a, const Grp<G>& grp, int p, bool act
     }
 }
 
+// Largest pipeline period of the cooperative classes (their rings hold P + 8
+// entries per warp in shared memory).
+constexpr int COOP_PMAX = 4088;
+
 // Launch helpers implemented by the kernel translation units.
 int launch_sw32(const SwArgs& a, bool tb, bool xd, int e_mode, bool queued, int grid, int wpb,
                 cudaStream_t stream);
@@ -384,5 +391,7 @@ int launch_sw16(const SwArgs& a, int cls, bool tb, bool xd, int e_mode, int grid
                 cudaStream_t stream);
 int sw32_smem_per_warp(int ring);
 int sw16_smem_per_warp(int cls, int ring);
+int launch_sw16_coop(const SwArgs& a, int cls, bool tb, bool xd, int e_mode, cudaStream_t stream);
+int sw16_coop_warps(int cls);
 
 }  // namespace gmf

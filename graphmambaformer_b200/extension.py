@@ -253,6 +253,8 @@ def fetch(out: SWOutputs, n: int) -> SWResult:
         raise RuntimeError("gmf_banded_sw: traceback workspace exhausted")
     if r.error_flags & _native.GMF_SWF_CAPACITY:
         raise RuntimeError("gmf_banded_sw: CIGAR output capacity exhausted")
+    if r.error_flags & _native.GMF_SWF_TIMEOUT:
+        raise RuntimeError("gmf_banded_sw: a bounded wait between cooperating warps gave up")
     return r
 
 

@@ -119,6 +119,8 @@ typedef struct {
 
 #define GMF_SWF_WORKSPACE 1u /* a pair's traceback did not fit the workspace */
 #define GMF_SWF_CAPACITY 2u  /* cigar_capacity exceeded */
+#define GMF_SWF_TIMEOUT 4u   /* a bounded wait between the warps sharing a pair gave up (that
+                                pair's result is unreliable); not expected in normal operation */
 
 /* Bytes of workspace gmf_banded_sw needs for a batch.  HOST arrays. */
 size_t gmf_banded_sw_workspace_bytes(int32_t n_pairs, const int32_t* query_len,

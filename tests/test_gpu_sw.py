@@ -93,6 +93,37 @@ def test_sw_wide_bands_match_oracle(ext):
     assert_sw_equal(res, want, label="wide")
 
 
+def test_cooperative_classes_match_oracle(ext):
+    """Long pairs with wide bands are shared by 2, 4 or 8 warps of one CTA
+    (strip by strip, the row above passed between warps through shared
+    memory).  Pairs sized for each of those classes, plus the one-warp cases
+    just below their thresholds, match the oracle bit for bit with x-drop off
+    and on and under each gap-tie mode (open > ext, open == ext, open < ext)."""
+    from graphmambaformer_b200 import synth
+    from oracle import oracle
+
+    rng = np.random.default_rng(31)
+    ref = synth.random_reference(400_000, rng)
+    qs, ts, hbs = [], [], []
+    #  (length, half band): C2 (P >= 264), C4 (P >= 528), C8 (P >= 1056), and
+    #  one-warp fallbacks (too few strips, or period below the C2 threshold)
+    for L, hb in ((2000, 150), (900, 200), (3000, 300), (4200, 264), (5000, 600), (6000, 1000),
+                  (500, 300), (200, 600), (3000, 128)):
+        for prof in (synth.ONT, synth.HIFI):
+            s = int(rng.integers(2000, 390_000 - L))
+            qs.append(synth.apply_errors(ref[s: s + L], prof, rng))
+            ts.append(ref[s - 150: s + L + 150])
+            hbs.append(hb)
+    ps = synth.PairSet.from_lists(qs, ts, np.array(hbs, np.int32), 150)
+    for params in ((2, 4, 4, 2, 0), (2, 4, 6, 2, 300), (2, 4, 4, 4, 0), (1, 3, 2, 3, 0)):
+        res = ext.align_pairs(ps, ext.sw_params(*params))
+        want = oracle.sw_batch(qs, ts, ps.half_band, ps.band_offset, *params, threads=8)
+        assert_sw_equal(res, want, label=str(params))
+        plain = ext.align_pairs(ps, ext.sw_params(*params), form="plain")
+        assert np.array_equal(res.score, plain.score) and all(
+            res.cigar(k) == plain.cigar(k) for k in range(len(ps))), params
+
+
 def test_sw_same_result_alone_and_in_the_mix(ext):
     from graphmambaformer_b200 import synth
 
