@@ -3,19 +3,24 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-One JSON line on rank 0.  The headline ``value`` is banded-SW GCUPS of the
-extension workload (in-band DP cells per second, traceback included) with
-inputs resident in HBM; ``e2e`` is the same metric through the public session
-API with host inputs (pinned H2D copy, kernel, D2H of scores, coordinates and
-CIGARs, every step); ``chain`` reports chaining anchors/s of the HiFi chaining
-workload the same two ways.  Workloads are seeded synthetic data (no public
+One JSON line on rank 0.  The headline ``value`` is banded-SW GCUPS (in-band
+DP cells per second, traceback and CIGARs included) of the batched form on
+the mixed-length extension workload: 100,000 pairs with log-normal lengths
+from 150 bp to 20 kb, Illumina / HiFi / ONT error profiles and bands growing
+with length from 32 to 432, inputs resident in HBM.  ``plain`` is the plain
+per-batch form (one warp per pair, int32 cells, one launch) on the same
+batch; ``e2e`` is the same metric through the public ``ExtensionSession``
+API with host inputs (pinned H2D copy, kernels, D2H of scores, coordinates
+and CIGARs, every step).  ``extension_150bp`` reports the 10,000-pair 150 bp
+workload the same two ways and ``chain`` the chaining anchors/s of the HiFi
+chaining workload.  Workloads are seeded synthetic data (no public
 dataset).  Multi-GPU runs are replicas: every rank aligns its own shard-sized
 copy of the workload (weak scaling, no collective on the data path); times
 are device-measured per rank and the max over ranks is reported.
 
 ``--impl reference`` times the reference algorithm's CPU restatement (the C
-oracle, all host cores) on the same workloads and prints the same line with
-``"impl": "reference"``.
+oracle, all host cores) on a bounded, length-stratified sample of the same
+workload and prints the same line with ``"impl": "reference"``.
 """
 
 from __future__ import annotations
@@ -45,11 +50,12 @@ def parse():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--workload", default="extension_pairs_150bp",
+    p.add_argument("--workload", default="extension_pairs_mixed",
                    choices=["extension_pairs_150bp", "extension_pairs_mixed"])
-    p.add_argument("--pairs", type=int, default=10_000)
+    p.add_argument("--pairs", type=int, default=0, help="pairs of the headline workload (0: its default)")
     p.add_argument("--chain-reads", type=int, default=5_000)
     p.add_argument("--no-chain", action="store_true")
+    p.add_argument("--no-150bp", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile-case", action="store_true",
                    help="small single-GPU case for ncu captures (no timing JSON)")
@@ -62,6 +68,8 @@ def parse():
 def sw_workload(name: str, n_pairs: int, seed: int):
     from graphmambaformer_b200 import synth
 
+    if not n_pairs:
+        n_pairs = 10_000 if name == "extension_pairs_150bp" else 100_000
     if name == "extension_pairs_150bp":
         ps = synth.extension_pairs_150bp(n_pairs=n_pairs, seed=seed)
         params = (2, 4, 4, 2, 0)
@@ -70,8 +78,10 @@ def sw_workload(name: str, n_pairs: int, seed: int):
     else:
         ps = synth.extension_pairs_mixed(n_pairs=n_pairs, seed=seed)
         params = (2, 4, 4, 2, 0)
-        desc = dict(workload=name, pairs=len(ps), read_len="lognormal 150-20000",
-                    half_band="32-500 (32 + 0.02 len)", scoring="2/4/4/2")
+        desc = dict(workload=name, pairs=len(ps), read_len="lognormal(7.0, 1.2) clipped to 150-20000",
+                    profiles="Illumina 1% sub / HiFi 0.1% / ONT 5% (60% indels), one third each",
+                    half_band="clip(32 + 0.02 len, 32, 500)", band_offset=32,
+                    scoring="match 2, mismatch 4, open 4, extend 2, x_drop off")
     desc["cells"] = ps.cells()
     return ps, params, desc
 
@@ -192,6 +202,34 @@ def load_traffic():
     return out
 
 
+def launches_per_call(max_half_band: int, traceback: bool) -> int:
+    """Kernels one gmf_banded_sw call launches: the classifier, one kernel per
+    pair class that can be populated (the cooperative classes only when the
+    widest band reaches their period range), and the deferred walk."""
+    W = 2 * max_half_band + 1
+    P = max(W + 2, 128)
+    P = (P + 3) & ~3
+    coop = sum(1 for pmin in (8 * 132, 4 * 132, 2 * 132) if P >= pmin)
+    return 1 + coop + 3 + 1 + (1 if traceback else 0)
+
+
+def time_device(fn, steps, stream, flush):
+    """Per-step device time of ``fn`` with CUDA events on ``stream``; the L2
+    is flushed (a 320 MB write) before every step, outside the events."""
+    import torch
+
+    out = []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return out
+
+
 # --------------------------------------------------------------------------- #
 # B200 arm
 # --------------------------------------------------------------------------- #
@@ -231,75 +269,66 @@ def run_b200(args):
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
         return float(t.item())
 
-    # ---- SW workload (each rank its own shard-sized replica) ----
-    ps, params, desc = sw_workload(args.workload, args.pairs, seed=1 + 1000 * rank)
-    sw_p = extension.sw_params(*params)
-    dp = extension.upload_pairs(ps, device)
-    out = extension.SWOutputs.allocate(dp, True)
-    ws = torch.empty(extension.workspace_bytes(dp, True), dtype=torch.uint8, device=device)
-    flush = torch.empty(320 * 1024 * 1024 // 4, dtype=torch.int32, device=device)  # > 126 MB L2
+    warm = max(args.warmup, 3)
     stream = torch.cuda.current_stream(device)
+    flush = torch.empty(320 * 1024 * 1024 // 4, dtype=torch.int32, device=device)  # > 126 MB L2
 
-    def sw_step():
-        extension.launch_banded_sw(dp, sw_p, True, out=out, workspace=ws, stream=stream)
+    def sw_leg(name, n_pairs, seed, clocks=None):
+        """Batched and plain device timing plus e2e of one SW workload."""
+        ps, params, desc = sw_workload(name, n_pairs, seed=seed)
+        sw_p = extension.sw_params(*params)
+        dp = extension.upload_pairs(ps, device)
+        out = extension.SWOutputs.allocate(dp, True)
+        ws = torch.empty(extension.workspace_bytes(dp, True), dtype=torch.uint8, device=device)
 
-    for _ in range(max(args.warmup, 3)):
-        sw_step()
-    torch.cuda.synchronize(device)
-    # correctness guard: the timed launch must report no workspace/capacity error
-    err = int(out.error_flags.item())
-    if err:
-        raise RuntimeError(f"SW kernel reported error flags {err}")
-    uuid = str(torch.cuda.get_device_properties(device).uuid) if hasattr(
-        torch.cuda.get_device_properties(device), "uuid") else ""
-    sampler = ClockSampler(uuid)
-    step_ms = []
-    with sampler:
+        def step(form):
+            return lambda: extension.launch_banded_sw(dp, sw_p, True, out=out, workspace=ws, stream=stream,
+                                                      form=form)
+
+        for _ in range(warm):
+            step("batched")()
+        torch.cuda.synchronize(device)
+        if int(out.error_flags.item()):  # the timed launches must report no workspace/capacity error
+            raise RuntimeError(f"SW kernels reported error flags {int(out.error_flags.item())}")
         barrier()
         torch.cuda.synchronize(device)
+        if clocks is not None:
+            with clocks:
+                b_ms = time_device(step("batched"), args.steps, stream, flush)
+        else:
+            b_ms = time_device(step("batched"), args.steps, stream, flush)
+        barrier()
+        for _ in range(warm):
+            step("plain")()
+        torch.cuda.synchronize(device)
+        p_ms = time_device(step("plain"), args.steps, stream, flush)
+        barrier()
+        sess = ExtensionSession(device, *params, traceback=True)
+        for _ in range(warm):
+            sess.align(ps)
+        barrier()
+        e_ms = []
         for _ in range(args.steps):
-            flush.zero_()  # evict L2 between timed steps (outside the timed events)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            sw_step()
-            e1.record(stream)
-            e1.synchronize()
-            step_ms.append(e0.elapsed_time(e1))
-        torch.cuda.synchronize(device)
+            t0 = time.perf_counter()
+            sess.align(ps)
+            e_ms.append((time.perf_counter() - t0) * 1e3)
         barrier()
-    # the plain per-batch form (one warp per pair, int32 cells) on the same batch
-    plain_ms = []
-    for _ in range(max(args.warmup, 3)):
-        extension.launch_banded_sw(dp, sw_p, True, out=out, workspace=ws, stream=stream, form="plain")
-    torch.cuda.synchronize(device)
-    for _ in range(args.steps):
-        flush.zero_()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        extension.launch_banded_sw(dp, sw_p, True, out=out, workspace=ws, stream=stream, form="plain")
-        e1.record(stream)
-        e1.synchronize()
-        plain_ms.append(e0.elapsed_time(e1))
-    cells_rank = desc["cells"]
-    ms_rank = float(np.mean(step_ms))
-    ms = max_over_ranks(ms_rank)
-    total_cells = sum_over_ranks(float(cells_rank))
-    gcups = total_cells / (ms * 1e-3) / 1e9
+        cells = float(desc["cells"])
+        total = sum_over_ranks(cells)
+        b = max_over_ranks(float(np.mean(b_ms)))
+        pl = max_over_ranks(float(np.mean(p_ms)))
+        e = max_over_ranks(float(np.mean(e_ms)))
+        del ws, out
+        return dict(ps=ps, params=params, desc=desc, cells=cells, total=total, batched_ms=b, plain_ms=pl,
+                    e2e_ms=e, rank_ms=float(np.mean(b_ms)), sess=sess,
+                    launches=launches_per_call(dp.max_half_band, True))
 
-    # ---- e2e through the session API (host inputs, pinned H2D, D2H) ----
-    sess = ExtensionSession(device, *params, traceback=True)
-    for _ in range(max(args.warmup, 3)):
-        sess.align(ps)
-    barrier()
-    e2e_ms = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        sess.align(ps)
-        e2e_ms.append((time.perf_counter() - t0) * 1e3)
-    barrier()
-    e2e_step = max_over_ranks(float(np.mean(e2e_ms)))
-    plain_step = max_over_ranks(float(np.mean(plain_ms)))
-    e2e_gcups = total_cells / (e2e_step * 1e-3) / 1e9
+    uuid = str(getattr(torch.cuda.get_device_properties(device), "uuid", ""))
+    sampler = ClockSampler(uuid)
+    head = sw_leg(args.workload, args.pairs, 1 + 1000 * rank, clocks=sampler)
+    small = None
+    if not args.no_150bp and args.workload != "extension_pairs_150bp":
+        small = sw_leg("extension_pairs_150bp", 0, 11 + 1000 * rank)
 
     # ---- chaining ----
     chain = None
@@ -308,19 +337,15 @@ def run_b200(args):
         cfg = ChainingConfig(max_lookback=50, max_gap=5000)
         da = chaining.upload_anchors(cb, device)
         cout = chaining.ChainOutputs.allocate(da, cfg.max_chains)
-        for _ in range(max(args.warmup, 3)):
+
+        def cstep():
             chaining.launch_chain_batch(da, cfg, out=cout, stream=stream)
+
+        for _ in range(warm):
+            cstep()
         torch.cuda.synchronize(device)
         barrier()
-        cms = []
-        for _ in range(args.steps):
-            flush.zero_()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            chaining.launch_chain_batch(da, cfg, out=cout, stream=stream)
-            e1.record(stream)
-            e1.synchronize()
-            cms.append(e0.elapsed_time(e1))
+        cms = time_device(cstep, args.steps, stream, flush)
         barrier()
         c_ms = max_over_ranks(float(np.mean(cms)))
         anchors_total = sum_over_ranks(float(cb.n_anchors))
@@ -348,37 +373,44 @@ def run_b200(args):
     if rank != 0:
         return None
 
-    # ---- roofline (rank 0, single-GPU kernel figures) ----
+    # ---- roofline (rank 0, single-GPU figures of the headline call) ----
     peaks, peak_src = load_peaks()
     ip = measure_int_peak(device)
     int_peak = ip["int32_add_max"]
+    cells_rank, ms_rank = head["cells"], head["rank_ms"]
     achieved_int = INT_OPS_PER_CELL * cells_rank / (ms_rank * 1e-3) / 1e12
     traffic = load_traffic()
     tpc = traffic.get("sw_bytes_per_cell")
+    ps = head["ps"]
     alg_bytes = TB_BYTES_PER_CELL * cells_rank + int(ps.query.size + ps.target.size)
+    gcups = head["total"] / (head["batched_ms"] * 1e-3) / 1e9
+    plain_gcups = head["total"] / (head["plain_ms"] * 1e-3) / 1e9
     line = {
         "metric": METRIC,
         "value": gcups,
         "unit": "GCUPS",
         "n_gpus": world,
         "steps": args.steps,
-        "warmup": max(args.warmup, 3),
-        "ms_per_step": ms,
+        "warmup": warm,
+        "ms_per_step": head["batched_ms"],
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "int32",
+        "dtype": "u16x2 / int32 (exact integer scores)",
         "data": "synthetic (seeded, reference simulator error model)",
-        "config": dict(desc, parallelism=f"replicas x{world}", l2="flushed between timed steps",
-                       traceback="on (CIGAR per pair)", kernel="gmf_banded_sw batched: device classifier + int16x2 work-queue kernels"),
-        "e2e": {"value": e2e_gcups, "unit": "GCUPS", "ms_per_step": e2e_step,
-                "h2d_bytes_per_step": sess.h2d_bytes, "d2h_bytes_per_step": sess.d2h_bytes,
+        "config": dict(head["desc"], parallelism=f"replicas x{world}", l2="flushed between timed steps",
+                       traceback="on (CIGAR per pair)",
+                       form="batched: device classifier, class kernels on side streams, deferred walk"),
+        "e2e": {"value": head["total"] / (head["e2e_ms"] * 1e-3) / 1e9, "unit": "GCUPS",
+                "ms_per_step": head["e2e_ms"], "h2d_bytes_per_step": head["sess"].h2d_bytes,
+                "d2h_bytes_per_step": head["sess"].d2h_bytes,
                 "timing": "wall clock around ExtensionSession.align (synchronous)"},
-        "plain": {"value": total_cells / (plain_step * 1e-3) / 1e9, "unit": "GCUPS",
-                  "ms_per_step": plain_step, "form": "gmf_banded_sw_plain: one warp per pair, int32, one launch",
-                  "batched_over_plain": plain_step / ms},
-        "gpu_launches": args.steps * 5,
-        "roofline": {"bound": "int", "achieved": achieved_int, "peak": int_peak, "unit": "Tops/s",
+        "plain": {"value": plain_gcups, "unit": "GCUPS", "ms_per_step": head["plain_ms"],
+                  "form": "gmf_banded_sw_plain: one warp per pair, int32 cells, one launch",
+                  "batched_over_plain": gcups / plain_gcups},
+        "gpu_launches": args.steps * head["launches"],
+        "roofline": {"bound": "int", "kernel": "gmf_banded_sw (all kernels of one call)",
+                     "achieved": achieved_int, "peak": int_peak, "unit": "Tops/s",
                      "frac": achieved_int / int_peak, "peak_source": "int32 add/max probe, this GPU",
                      "ops_per_cell": INT_OPS_PER_CELL,
                      "traffic": (tpc * cells_rank) if tpc else None},
@@ -389,10 +421,19 @@ def run_b200(args):
         "int_probe_tops": ip,
         "clocks": sampler.summary(),
     }
+    if small:
+        line["extension_150bp"] = {
+            "value": small["total"] / (small["batched_ms"] * 1e-3) / 1e9, "unit": "GCUPS",
+            "ms_per_step": small["batched_ms"], "config": small["desc"],
+            "plain": small["total"] / (small["plain_ms"] * 1e-3) / 1e9,
+            "e2e": {"value": small["total"] / (small["e2e_ms"] * 1e-3) / 1e9, "unit": "GCUPS",
+                    "h2d_bytes_per_step": small["sess"].h2d_bytes,
+                    "d2h_bytes_per_step": small["sess"].d2h_bytes},
+            "gpu_launches_per_step": small["launches"]}
     if chain:
         line["chain"] = chain
     if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(ps, params, cells_rank)
+        line["cpu_baseline"] = cpu_baseline(ps, head["params"])
     return line
 
 
@@ -406,49 +447,66 @@ def host_threads() -> int:
         return os.cpu_count() or 1
 
 
-def cpu_baseline(ps, params, cells, sample_pairs: int = 10_000) -> dict:
-    from oracle import oracle
-
-    n = min(sample_pairs, len(ps))
-    qs = [ps.q(b) for b in range(n)]
-    ts = [ps.t(b) for b in range(n)]
+def stratified_sample(ps, max_cells: float, seed: int = 0) -> np.ndarray:
+    """Pair indices of a sample of ``ps`` covering every length decile in
+    proportion, about ``max_cells`` in-band cells in total."""
     from graphmambaformer_b200.synth import band_cells
 
-    cs = int(band_cells(ps.query_len[:n], ps.target_len[:n], ps.half_band[:n], ps.band_offset[:n]).sum())
-    th = host_threads()
+    cells = band_cells(ps.query_len, ps.target_len, ps.half_band, ps.band_offset).astype(np.float64)
+    if cells.sum() <= max_cells:
+        return np.arange(len(ps))
+    rng = np.random.default_rng(seed)
+    frac = max_cells / cells.sum()
+    order = np.argsort(ps.query_len, kind="stable")
+    picks = []
+    for dec in np.array_split(order, 10):
+        k = max(1, int(round(len(dec) * frac)))
+        picks.append(rng.choice(dec, size=min(k, len(dec)), replace=False))
+    return np.sort(np.concatenate(picks))
+
+
+def oracle_sw_rate(ps, params, idx, threads):
+    """GCUPS of the C oracle (the reference algorithm, SW + traceback) on the
+    pairs ``idx`` of ``ps``; returns (gcups, cells, seconds)."""
+    from graphmambaformer_b200.synth import band_cells
+    from oracle import oracle
+
+    qs = [ps.q(int(b)) for b in idx]
+    ts = [ps.t(int(b)) for b in idx]
+    cs = float(band_cells(ps.query_len[idx], ps.target_len[idx], ps.half_band[idx], ps.band_offset[idx]).sum())
     t0 = time.perf_counter()
-    oracle.sw_batch(qs, ts, ps.half_band[:n], ps.band_offset[:n], *params, threads=th)
+    oracle.sw_batch(qs, ts, ps.half_band[idx], ps.band_offset[idx], *params, threads=threads)
     dt = time.perf_counter() - t0
-    return {"value": cs / dt / 1e9, "unit": "GCUPS", "cores": th, "kind": "port",
-            "sample": f"{n} pairs ({cs} cells) of the same workload, SW + traceback, C oracle"}
+    return cs / dt / 1e9, cs, dt
+
+
+def cpu_baseline(ps, params, max_cells: float = 6e9) -> dict:
+    th = host_threads()
+    idx = stratified_sample(ps, max_cells)
+    gcups, cs, dt = oracle_sw_rate(ps, params, idx, th)
+    return {"value": gcups, "unit": "GCUPS", "cores": th, "kind": "port",
+            "sample": f"{len(idx)} pairs ({cs:.3g} cells, every length decile) of the same workload, "
+                      f"SW + traceback, C restatement of the reference, {dt:.1f} s"}
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
-    from oracle import oracle
-
     ps, params, desc = sw_workload(args.workload, args.pairs, seed=1)
     th = host_threads()
-    n = len(ps)
-    if desc["workload"] != "extension_pairs_150bp":
-        n = min(n, 2000)
-    qs = [ps.q(b) for b in range(n)]
-    ts = [ps.t(b) for b in range(n)]
-    from graphmambaformer_b200.synth import band_cells
-
-    cells = int(band_cells(ps.query_len[:n], ps.target_len[:n], ps.half_band[:n], ps.band_offset[:n]).sum())
+    idx = stratified_sample(ps, 2e9)
+    warm_idx = idx[:: max(1, len(idx) // 20)]
     for _ in range(max(args.warmup, 3) if args.warmup else 0):
-        oracle.sw_batch(qs[:200], ts[:200], ps.half_band[:200], ps.band_offset[:200], *params, threads=th)
-    times = []
+        oracle_sw_rate(ps, params, warm_idx[:4], th)
+    times, cells = [], 0.0
     for _ in range(args.steps):
-        t0 = time.perf_counter()
-        oracle.sw_batch(qs, ts, ps.half_band[:n], ps.band_offset[:n], *params, threads=th)
-        times.append(time.perf_counter() - t0)
+        _, cells, dt = oracle_sw_rate(ps, params, idx, th)
+        times.append(dt)
     ms = float(np.mean(times)) * 1e3
     gcups = cells / (ms * 1e-3) / 1e9
-    sample = f"{n} pairs ({cells} cells) per step, SW + traceback, C restatement of the reference"
+    sample = (f"{len(idx)} pairs ({cells:.3g} cells, every length decile) per step, SW + traceback, "
+              f"C restatement of the reference")
     line = {
         "impl": "reference", "metric": METRIC, "value": gcups, "unit": "GCUPS", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
@@ -458,6 +516,8 @@ def run_reference(args):
         "e2e": {"value": gcups, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     if not args.no_chain:
+        from oracle import oracle
+
         cb, cdesc = chain_workload(min(args.chain_reads, 1000), seed=2)
         lut = oracle.penalty_lut(5000, 6.0, 0.05, 0.5)
         t0 = time.perf_counter()
@@ -470,12 +530,13 @@ def run_reference(args):
 
 
 def profile_case(args):
-    """A small case for ncu: 2,000 pairs of the 150 bp workload, 3 launches."""
+    """A small single-GPU case for ncu captures: 2,000 pairs of the chosen
+    workload, 3 launches of the batched form."""
     import torch
 
     from graphmambaformer_b200 import extension
 
-    ps, params, _ = sw_workload(args.workload, 2000, seed=1)
+    ps, params, _ = sw_workload(args.workload, args.pairs or 2000, seed=1)
     dp = extension.upload_pairs(ps, "cuda:0")
     for _ in range(3):
         extension.launch_banded_sw(dp, extension.sw_params(*params), True)

@@ -409,6 +409,10 @@ __device__ void sw16_group(const SwArgs& a, int p, const Grp<L>& grp, uint32_t* 
         a.t_end[p] = te;
     }
     if (!TB) return;
+    if (a.defer_walk) {  // the traceback walk runs later, in sw_walk_kernel
+        if (active && k == 0) record_walk(a, p, bits, L);
+        return;
+    }
 
     RunWriter rw;
     uint32_t* runs = ws_alloc<L>(a, grp, (unsigned long long)qe + te + 1, active && bh > 0);
@@ -632,6 +636,10 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, volatile
         a.t_end[p] = te;
     }
     if (!TB) return;
+    if (a.defer_walk) {  // the traceback walk runs later, in sw_walk_kernel
+        if (lane == 0) record_walk(a, p, bits, L);
+        return;
+    }
     RunWriter rw;
     uint32_t* runs = ws_alloc<32>(a, grp, (unsigned long long)qe + te + 1, bh > 0);
     const bool runs_ok = bh == 0 || runs != nullptr;
@@ -698,6 +706,59 @@ int launch_sw16_coop(const SwArgs& a, int cls, bool tb, bool xd, int e_mode, cud
     if (cls == CLS_I16_C2) return launch_coop_x<2>(a, tb, xd, e_mode, stream);
     if (cls == CLS_I16_C4) return launch_coop_x<4>(a, tb, xd, e_mode, stream);
     return launch_coop_x<8>(a, tb, xd, e_mode, stream);
+}
+
+// ---------------------------------------------------------------------------
+// Deferred traceback walk of the batched form: one warp per pair, longest
+// pairs first, after every DP kernel has stored its bits.  Running the walks
+// as one wide kernel hides their scattered loads behind many warps and keeps
+// the warps of the cooperative classes from idling while one warp walks.
+// ---------------------------------------------------------------------------
+template <class Lay>
+__device__ void walk_pair(const SwArgs& a, const Grp<32>& grp, int p, const PairGeo& G, const Lay& lay) {
+    const int bh = a.score[p], qe = a.q_end[p], te = a.t_end[p];
+    RunWriter rw;
+    uint32_t* runs = ws_alloc<32>(a, grp, (unsigned long long)qe + te + 1, bh > 0);
+    const bool runs_ok = bh == 0 || runs != nullptr;
+    if (!runs_ok && grp.k == 0) atomicOr(a.err, (int)GMF_SWF_WORKSPACE);
+    rw.init(runs);
+    int qs = 0, ts = 0;
+    walk<32>(grp, lay, G, qe, te, runs_ok && bh > 0, rw, qs, ts);
+    finish_cigar<32>(a, grp, p, true, rw, runs_ok, qs, ts);
+}
+
+__global__ void __launch_bounds__(128) sw_walk_kernel(SwArgs a) {
+    const int lane = threadIdx.x & 31;
+    Grp<32> grp(lane);
+    for (;;) {
+        unsigned long long idx = 0;
+        if (lane == 0) idx = atomicAdd(&a.counters[1], 1ull);
+        idx = __shfl_sync(FULL_MASK, idx, 0);
+        if (idx >= (unsigned long long)a.n_pairs) break;
+        const int p = a.order ? a.order[idx] : (int)idx;
+        const int tag = a.tb_tag[p];
+        if (tag < 0) continue;  // no traceback: empty pair, bad band or workspace exhausted
+        const PairGeo G = load_geo(a, p);
+        const uint32_t* bits = a.pool + a.tb_base[p];
+        if (tag == 0) {
+            walk_pair(a, grp, p, G, Layout32{bits, imax(64, G.W + 1), G.W, G.qlen});
+        } else if (tag == 8) {
+            walk_pair(a, grp, p, G, Layout16<8>{bits, sw16_period(G.W, 8), G.W, G.qlen});
+        } else if (tag == 16) {
+            walk_pair(a, grp, p, G, Layout16<16>{bits, sw16_period(G.W, 16), G.W, G.qlen});
+        } else {
+            walk_pair(a, grp, p, G, Layout16<32>{bits, sw16_period(G.W, 32), G.W, G.qlen});
+        }
+    }
+}
+
+int launch_sw_walk(const SwArgs& a, cudaStream_t stream) {
+    int dev = 0, sms = 0, per_sm = 0;
+    GMF_CUDA_TRY(cudaGetDevice(&dev));
+    GMF_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    GMF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sw_walk_kernel, 128, 0));
+    sw_walk_kernel<<<sms * (per_sm > 0 ? per_sm : 1), 128, 0, stream>>>(a);
+    return cuda_status(cudaGetLastError());
 }
 
 int sw16_smem_per_warp(int cls, int ring) {

@@ -48,17 +48,6 @@ __host__ __device__ inline unsigned long long sw32_tb_words(int qlen, int W) {
     return (unsigned long long)((last >> 3) + 1) * 32ull;
 }
 
-struct Layout32 {
-    const uint32_t* bits;
-    int P, W, qlen;
-    __device__ uint32_t nib(int i, int d) const {
-        if (d < 0 || d >= W || i < 1 || i > qlen) return 0u;
-        const int v = (i - 1) & 31, s = (i - 1) >> 5;
-        const long long g = (long long)s * P + 2 * v + d;
-        return (bits[(g >> 3) * 32 + v] >> ((int)(g & 7) * 4)) & 15u;
-    }
-};
-
 template <bool TB, bool XD, int EM>
 __device__ void sw32_pair(const SwArgs& a, int p, const Grp<32>& grp, int2* ring) {
     PairGeo G = load_geo(a, p);
@@ -198,6 +187,10 @@ __device__ void sw32_pair(const SwArgs& a, int p, const Grp<32>& grp, int2* ring
         a.t_end[p] = te;
     }
     if (!TB) return;
+    if (a.defer_walk) {  // the traceback walk runs later, in sw_walk_kernel
+        if (lane == 0) record_walk(a, p, bits, 0);
+        return;
+    }
 
     RunWriter rw;
     uint32_t* runs = ws_alloc<32>(a, grp, (unsigned long long)qe + te + 1, bh > 0);

@@ -15,6 +15,7 @@
 // computes the same integer DP and the same traceback decisions.
 
 #include <algorithm>
+#include <mutex>
 
 #include "sw_common.cuh"
 
@@ -88,8 +89,43 @@ __global__ void sw_classify_kernel(SwArgs a) {
 
 static size_t round_up(size_t x, size_t m) { return (x + m - 1) / m * m; }
 
+// Queue heads and counts, the class lists, and the per-pair traceback
+// location (base word, layout tag) the deferred walk reads.
 static size_t queue_bytes(int n_pairs) {
-    return round_up(2 * N_CLASSES * sizeof(int32_t), 256) + round_up((size_t)N_CLASSES * n_pairs * 4, 256);
+    return round_up(2 * N_CLASSES * sizeof(int32_t), 256) + round_up((size_t)N_CLASSES * n_pairs * 4, 256) +
+           round_up((size_t)n_pairs * 8, 256) + round_up((size_t)n_pairs * 4, 256);
+}
+
+// Side streams of the batched form, one per pair class, created once per
+// device.  The class kernels are forked onto them from the caller's stream
+// and joined back before the walk, so a class whose long pairs are draining
+// shares the GPU with the next class instead of idling it.
+constexpr int N_SIDE = N_CLASSES;
+struct SideStreams {
+    cudaStream_t s[N_SIDE];
+    cudaEvent_t fork;
+    cudaEvent_t join[N_SIDE];
+    bool ready;
+};
+constexpr int kMaxSideDevices = 64;
+std::mutex g_side_mu;  // guards creation and every fork/launch/join sequence
+SideStreams g_side[kMaxSideDevices];
+
+static int side_streams(SideStreams** out) {
+    int dev = 0;
+    GMF_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxSideDevices) return GMF_ERR_LIMIT;
+    SideStreams& ss = g_side[dev];
+    if (!ss.ready) {
+        for (int i = 0; i < N_SIDE; ++i) {
+            GMF_CUDA_TRY(cudaStreamCreateWithFlags(&ss.s[i], cudaStreamNonBlocking));
+            GMF_CUDA_TRY(cudaEventCreateWithFlags(&ss.join[i], cudaEventDisableTiming));
+        }
+        GMF_CUDA_TRY(cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming));
+        ss.ready = true;
+    }
+    *out = &ss;
+    return GMF_OK;
 }
 
 static int ring_entries(int d_max) {
@@ -213,6 +249,12 @@ static int sw_prepare(const gmf_pairs* pairs, const gmf_sw_params* params, const
     a.counters = (unsigned long long*)w;
     a.queue = (int32_t*)(w + 256);
     a.lists = (int32_t*)(w + 256 + round_up(2 * N_CLASSES * sizeof(int32_t), 256));
+    char* tb = (char*)a.lists + round_up((size_t)N_CLASSES * pairs->n_pairs * 4, 256);
+    a.tb_base = (unsigned long long*)tb;
+    a.tb_tag = (int32_t*)(tb + round_up((size_t)pairs->n_pairs * 8, 256));
+    a.defer_walk = 0;
+    if (pairs->n_pairs > 0)
+        GMF_CUDA_TRY(cudaMemsetAsync(a.tb_tag, 0xFF, (size_t)pairs->n_pairs * 4, stream));
     a.pool = (uint32_t*)(w + 256 + qb);
     a.pool_cap = (workspace_bytes - 256 - qb) / 4;
     return GMF_OK;
@@ -230,15 +272,27 @@ extern "C" int gmf_banded_sw(const gmf_pairs* pairs, const gmf_sw_params* params
     const bool tb = res->cigar != nullptr;
     const bool xd = params->x_drop > 0;
     const int em = e_mode_of(params);
+    a.defer_walk = tb ? 1 : 0;
 
     const int cls_blocks = std::min((pairs->n_pairs + 255) / 256, di.sms * 4);
     sw_classify_kernel<<<cls_blocks, 256, 0, stream>>>(a);
     GMF_CUDA_TRY(cudaGetLastError());
 
     const int Wmax = 2 * pairs->max_half_band + 1;
-    // cooperative classes first (the longest pairs), each with a ring of
-    // P + 8 entries per warp for the largest period the class can hold
     const int Pmax = sw16_period(Wmax, 32);
+    // every class kernel goes to its own side stream, longest classes first
+    std::lock_guard<std::mutex> lock(g_side_mu);
+    SideStreams* ss = nullptr;
+    GMF_TRY(side_streams(&ss));
+    GMF_CUDA_TRY(cudaEventRecord(ss->fork, stream));
+    int used = 0;
+    auto next_stream = [&](cudaStream_t* out) -> int {
+        GMF_CUDA_TRY(cudaStreamWaitEvent(ss->s[used], ss->fork, 0));
+        *out = ss->s[used++];
+        return GMF_OK;
+    };
+    // cooperative classes, each with a ring of P + 8 entries per warp for the
+    // largest period the class can hold
     const int coop_cls[3] = {CLS_I16_C8, CLS_I16_C4, CLS_I16_C2};
     const int coop_pmin[3] = {8 * 132, 4 * 132, 2 * 132};
     const int coop_pcap[3] = {COOP_PMAX, 8 * 132 - 4, 4 * 132 - 4};
@@ -247,25 +301,39 @@ extern "C" int gmf_banded_sw(const gmf_pairs* pairs, const gmf_sw_params* params
         SwArgs ac = a;
         ac.ring = ring_entries(std::min(Pmax, coop_pcap[c]) + 7);
         if ((size_t)sw16_coop_warps(coop_cls[c]) * ac.ring * 4 > (size_t)di.smem_optin) return GMF_ERR_LIMIT;
-        GMF_TRY(launch_sw16_coop(ac, coop_cls[c], tb, xd, em, stream));
+        cudaStream_t s;
+        GMF_TRY(next_stream(&s));
+        GMF_TRY(launch_sw16_coop(ac, coop_cls[c], tb, xd, em, s));
     }
-    // one-warp and shared-warp classes (a class only ever holds pairs up to its own band limit)
+    // one-warp and shared-warp classes (a class only ever holds pairs up to
+    // its own band limit), widest first
     const int cls_wmax[3] = {std::min(Wmax, 61), std::min(Wmax, 125), Wmax};
     const int lanes[3] = {8, 16, 32};
-    for (int c = 0; c < 3; ++c) {
+    for (int c = 2; c >= 0; --c) {
         const int L = lanes[c];
         SwArgs ac = a;
         ac.ring = ring_entries(std::max(3, sw16_period(cls_wmax[c], L) - 4 * L - 1));
         const int wpb = warps_per_block((size_t)sw16_smem_per_warp(c, ac.ring), di);
         if (wpb == 0) return GMF_ERR_LIMIT;
         const int grid = di.sms * std::max(1, 16 / wpb);
-        GMF_TRY(launch_sw16(ac, c, tb, xd, em, grid, wpb, stream));
+        cudaStream_t s;
+        GMF_TRY(next_stream(&s));
+        GMF_TRY(launch_sw16(ac, c, tb, xd, em, grid, wpb, s));
     }
     SwArgs a32 = a;
     a32.ring = ring_entries(std::max(64, Wmax + 1) - 64);
     const int wpb = warps_per_block((size_t)sw32_smem_per_warp(a32.ring), di);
     if (wpb == 0) return GMF_ERR_LIMIT;
-    return launch_sw32(a32, tb, xd, em, true, di.sms * std::max(1, 12 / wpb), wpb, stream);
+    {
+        cudaStream_t s;
+        GMF_TRY(next_stream(&s));
+        GMF_TRY(launch_sw32(a32, tb, xd, em, true, di.sms * std::max(1, 12 / wpb), wpb, s));
+    }
+    for (int i = 0; i < used; ++i) {
+        GMF_CUDA_TRY(cudaEventRecord(ss->join[i], ss->s[i]));
+        GMF_CUDA_TRY(cudaStreamWaitEvent(stream, ss->join[i], 0));
+    }
+    return tb ? launch_sw_walk(a, stream) : GMF_OK;
 }
 
 extern "C" int gmf_banded_sw_plain(const gmf_pairs* pairs, const gmf_sw_params* params,

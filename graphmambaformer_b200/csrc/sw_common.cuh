@@ -54,7 +54,30 @@ struct SwArgs {
     int32_t* cigar_len;
     unsigned long long* cigar_used;
     int32_t* err;
+    int32_t defer_walk;              // batched form: DP kernels leave the walk to sw_walk_kernel
+    unsigned long long* tb_base;     // per pair: first traceback word (pool offset)
+    int32_t* tb_tag;                 // per pair: traceback layout (0 int32, L for 16x2), -1 none
 };
+
+// Traceback-bit layout of the int32 form: one 32-bit word per lane per 8
+// steps, 4 bits per step; virtual lane v of strip s handles slot d at step
+// s*P + 2v + d.
+struct Layout32 {
+    const uint32_t* bits;
+    int P, W, qlen;
+    __device__ uint32_t nib(int i, int d) const {
+        if (d < 0 || d >= W || i < 1 || i > qlen) return 0u;
+        const int v = (i - 1) & 31, s = (i - 1) >> 5;
+        const long long g = (long long)s * P + 2 * v + d;
+        return (bits[(g >> 3) * 32 + v] >> ((int)(g & 7) * 4)) & 15u;
+    }
+};
+
+// Where the deferred walk of pair p finds its traceback bits.
+__device__ __forceinline__ void record_walk(const SwArgs& a, int p, const uint32_t* bits, int tag) {
+    a.tb_base[p] = (unsigned long long)(bits - a.pool);
+    a.tb_tag[p] = tag;
+}
 
 // Pipeline period of the 16x2 form: steps per strip of 2L rows, a multiple of
 // 4 so that rows start on 4-step chunk boundaries.
@@ -392,6 +415,7 @@ int launch_sw16(const SwArgs& a, int cls, bool tb, bool xd, int e_mode, int grid
 int sw32_smem_per_warp(int ring);
 int sw16_smem_per_warp(int cls, int ring);
 int launch_sw16_coop(const SwArgs& a, int cls, bool tb, bool xd, int e_mode, cudaStream_t stream);
+int launch_sw_walk(const SwArgs& a, cudaStream_t stream);
 int sw16_coop_warps(int cls);
 
 }  // namespace gmf
