@@ -59,6 +59,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile-case", action="store_true",
                    help="small single-GPU case for ncu captures (no timing JSON)")
+    p.add_argument("--profile-longest", type=int, default=0,
+                   help="with --profile-case: the N largest pairs (by DP area) of the workload")
     return p.parse_args()
 
 
@@ -531,12 +533,17 @@ def run_reference(args):
 
 def profile_case(args):
     """A small single-GPU case for ncu captures: 2,000 pairs of the chosen
-    workload, 3 launches of the batched form."""
+    workload (or its N largest pairs), 3 launches of the batched form."""
     import torch
 
     from graphmambaformer_b200 import extension
 
-    ps, params, _ = sw_workload(args.workload, args.pairs or 2000, seed=1)
+    if args.profile_longest:
+        ps, params, _ = sw_workload(args.workload, args.pairs, seed=1)
+        area = ps.query_len.astype(np.int64) * (2 * ps.half_band.astype(np.int64) + 1)
+        ps = ps.subset(np.sort(np.argsort(-area, kind="stable")[: args.profile_longest]))
+    else:
+        ps, params, _ = sw_workload(args.workload, args.pairs or 2000, seed=1)
     dp = extension.upload_pairs(ps, "cuda:0")
     for _ in range(3):
         extension.launch_banded_sw(dp, extension.sw_params(*params), True)

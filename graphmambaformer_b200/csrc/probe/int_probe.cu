@@ -9,6 +9,8 @@
 //   permute / funnel shift) so their cost relative to one int32 op is known
 //   kinds 7-9 time the unsigned 16x2 forms (max, min, three-way max, DPX
 //   add-max) the biased-unsigned SW cells use
+//   kinds 10-14 time single forms against a plain add / xor pair (kind 12):
+//   packed add / sub, byte permute, DPX add-min + three-way max, multiply-add
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -53,6 +55,21 @@ __global__ void int_probe_kernel(int iters, int a, int b, int* out) {
             } else if (KIND == 9) {  // DPX unsigned 16x2 add-max
                 x[k] = (int)__viaddmax_u16x2((unsigned)x[k], (unsigned)a, (unsigned)y[k]);
                 y[k] = (int)__viaddmax_u16x2((unsigned)y[k], (unsigned)b, (unsigned)x[k]);
+            } else if (KIND == 10) {  // packed 16x2 add / sub alone
+                x[k] = (int)__vadd2((unsigned)x[k], (unsigned)a);
+                y[k] = (int)__vsub2((unsigned)y[k], (unsigned)x[k]);
+            } else if (KIND == 11) {  // byte permutes alone
+                x[k] = (int)__byte_perm((unsigned)x[k], (unsigned)y[k], 0x5410);
+                y[k] = (int)__byte_perm((unsigned)y[k], (unsigned)x[k], 0x7632) + a;
+            } else if (KIND == 12) {  // plain add / xor (reference pair)
+                x[k] = x[k] + a;
+                y[k] = y[k] ^ x[k];
+            } else if (KIND == 13) {  // DPX add-min (0/1 flags) and three-way max
+                x[k] = (int)__viaddmin_u16x2((unsigned)x[k], 0u, (unsigned)y[k]);
+                y[k] = (int)__vimax3_u16x2((unsigned)y[k], (unsigned)x[k], (unsigned)a);
+            } else if (KIND == 14) {  // multiply-add
+                x[k] = x[k] * a + y[k];
+                y[k] = y[k] * b + x[k];
             } else {  // byte permute + funnel shift (exchange and bit packing)
                 x[k] = (int)__byte_perm((unsigned)x[k], (unsigned)y[k], 0x5432) + a;
                 y[k] = (int)__funnelshift_r((unsigned)y[k], (unsigned)x[k], 8);
@@ -80,7 +97,12 @@ extern "C" int gmf_probe_int(int kind, int blocks, int threads, int iters, int* 
         case 6: int_probe_kernel<6><<<blocks, threads, 0, s>>>(iters, 3, 5, out); break;
         case 7: int_probe_kernel<7><<<blocks, threads, 0, s>>>(iters, 0x00030003, 0x00050005, out); break;
         case 8: int_probe_kernel<8><<<blocks, threads, 0, s>>>(iters, 0x00030003, 0x00050005, out); break;
-        default: int_probe_kernel<9><<<blocks, threads, 0, s>>>(iters, 0x00030003, 0x00050005, out); break;
+        case 9: int_probe_kernel<9><<<blocks, threads, 0, s>>>(iters, 0x00030003, 0x00050005, out); break;
+        case 10: int_probe_kernel<10><<<blocks, threads, 0, s>>>(iters, 0x00030003, 0x00050005, out); break;
+        case 11: int_probe_kernel<11><<<blocks, threads, 0, s>>>(iters, 3, 5, out); break;
+        case 12: int_probe_kernel<12><<<blocks, threads, 0, s>>>(iters, 3, 5, out); break;
+        case 13: int_probe_kernel<13><<<blocks, threads, 0, s>>>(iters, 0x00030003, 0x00050005, out); break;
+        default: int_probe_kernel<14><<<blocks, threads, 0, s>>>(iters, 3, 5, out); break;
     }
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }

@@ -11,9 +11,9 @@
 // with smax = match * (min(qlen, tlen) + 1).  The classifier sends a pair here
 // only when smax + Z + 2*pmax + 64 <= 65535, so all cells are exact unsigned
 // 16-bit integers and the local-alignment floor is a three-way max with Z.
-// Only full-rate instructions are used: __vadd2 / __vsub2, the DPX
-// __viaddmax_u16x2 / __viaddmin_u16x2 / __vimax3_u16x2, byte permutes, funnel
-// shifts and 32-bit integer ops.  Comparisons are differences of values known
+// The step uses the DPX __viaddmax_u16x2 / __viaddmin_u16x2 / __vimax3_u16x2,
+// byte permutes, funnel shifts and plain 32-bit integer ops (packed adds and
+// subtracts that cannot carry across halves are 32-bit adds).  Comparisons are differences of values known
 // to be ordered (H >= M >= diag, H >= F, F >= fa, E >= ea, E >= eb), turned
 // into 0/1 flags with min(x, 1).
 //
@@ -88,7 +88,7 @@ __device__ __forceinline__ unsigned tsel(int u) {
 // Per-lane DP state carried from step to step.
 struct Cells16 {
     unsigned hv, fv, hd, ml, el;  // H / F of the row above (this and the previous slot), M / E on the left
-    unsigned ma, mb;              // slot - band_lo, band_hi - slot per half (negative = out of band)
+    unsigned ma, mb;              // 32768 + slot - band_lo, 32768 + band_hi - slot per half (bit 15 set: in)
     unsigned qp;                  // query codes of the two rows (0x100 = never matches)
     unsigned acc;                 // traceback nibbles of the chunk
 };
@@ -117,8 +117,8 @@ __device__ __forceinline__ void cells_init(Cells16& c, const K16& K) {
     c.hd = K.Z2;
     c.ml = K.NEG2;
     c.el = K.NEG2;
-    c.ma = pack16(-30000, -30000);
-    c.mb = 0u;
+    c.ma = pack16(2768, 2768);  // out of band until the lane's first row starts
+    c.mb = pack16(20000, 20000);
     c.qp = 0x01000100u;
     c.acc = 0u;
 }
@@ -176,8 +176,8 @@ __device__ __forceinline__ void row_start16(Cells16& c, int row, int j0, int qle
     const int hi0 = row <= qlen ? imax(imin(W - 1, tlen - j0), -1) : -1;
     const int lo1 = imin(imax(2, 2 - j0), 32000);
     const int hi1 = row + 1 <= qlen ? imax(imin(W + 1, tlen - j0 + 1), -1) : -1;
-    c.ma = pack16(-1 - lo0, -1 - lo1);
-    c.mb = pack16(hi0 + 1, hi1 + 1);
+    c.ma = pack16(32768 - 1 - lo0, 32768 - 1 - lo1);
+    c.mb = pack16(32768 + hi0 + 1, 32768 + hi1 + 1);
 }
 
 // Four pipeline steps of one lane.  The first lane of the group takes its
@@ -189,36 +189,43 @@ __device__ __forceinline__ void chunk16(Cells16& c, const K16& K, const Grp<L>& 
                                         unsigned (&hk)[4], unsigned (&pko)[4]) {
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
+        // Packed adds and subtracts below are plain 32-bit operations: every
+        // operand half is a biased value >= pmax, and every difference is
+        // taken between values known to be ordered, so no half borrows or
+        // carries into the other (a 16x2 __vadd2 / __vsub2 costs about three
+        // instructions on this part).
         const unsigned tp = prmt(tw, tpv, tsel(u));
         const unsigned mis = flag2(c.qp ^ tp);  // 0: match, 1: mismatch
-        const unsigned diag = __vadd2(c.hd, __vsub2(K.MATCH2, mis * K.MX));
-        const unsigned fa = __vsub2(c.hv, K.GO2);
+        const unsigned diag = c.hd + K.MATCH2 - mis * K.MX;
+        const unsigned fa = c.hv - K.GO2;
         unsigned F = __viaddmax_u16x2(c.fv, K.NGE2, fa);  // max(F above - ext, H above - open)
         unsigned M = __vimax3_u16x2(diag, F, K.Z2);
-        const unsigned ea = __vsub2(c.ml, K.GO2);
+        const unsigned ea = c.ml - K.GO2;
         unsigned E = __viaddmax_u16x2(c.el, K.NGE2, ea);
         unsigned H = umax2(M, E);
         if (TB) {
             const unsigned nz = __viaddmin_u16x2(H, K.NZ2, ONE2);  // H > 0
-            const unsigned n1 = flag2(__vsub2(H, diag));           // H != diag
-            const unsigned n2 = flag2(__vsub2(H, F));              // H != F
-            const unsigned fc = flag2(__vsub2(F, fa));             // F extends
+            const unsigned n1 = flag2(H - diag);                   // H != diag (H >= diag)
+            const unsigned n2 = flag2(H - F);                      // H != F (H >= F)
+            const unsigned fc = flag2(F - fa);                     // F extends (F >= fa)
             unsigned ec = 0u;                                      // E extends
-            if (EM == 0) ec = flag2(__vsub2(E, ea));
-            if (EM == 2) ec = flag2(__vsub2(E, __vsub2(c.el, K.GE2))) ^ ONE2;
+            if (EM == 0) ec = flag2(E - ea);
+            if (EM == 2) ec = flag2(E - (c.el - K.GE2)) ^ ONE2;
             const unsigned b0 = nz & (~n1 | n2);  // diagonal or E, when H > 0
             const unsigned b1 = nz & n1;          // F or E
             const unsigned x = b0 + 2u * b1 + 4u * fc + 8u * ec;
             c.acc = u == 0 ? x : c.acc * 16u + x;
         }
-        // in-band mask: slot - lo >= 0 and hi - slot >= 0 per half
-        c.ma = __vadd2(c.ma, ONE2);
-        c.mb = __vsub2(c.mb, ONE2);
-        const unsigned m = prmt(c.ma | c.mb, 0u, 0xBB99u);  // 0xFFFF per out-of-band half
-        H = (H & ~m) | (K.Z2 & m);
-        F = (F & ~m) | (K.NEG2 & m);
-        M = (M & ~m) | (K.NEG2 & m);
-        E = (E & ~m) | (K.NEG2 & m);
+        // in-band mask: slot - lo >= 0 and hi - slot >= 0 per half, kept as
+        // counters biased by 32768 (they never leave [0, 65535], so plain
+        // adds suffice); bit 15 of both set = in band
+        c.ma += ONE2;
+        c.mb -= ONE2;
+        const unsigned m = prmt(c.ma & c.mb, 0u, 0xBB99u);  // 0xFFFF per in-band half
+        H = (H & m) | (K.Z2 & ~m);
+        F = (F & m) | (K.NEG2 & ~m);
+        M = (M & m) | (K.NEG2 & ~m);
+        E = (E & m) | (K.NEG2 & ~m);
         const unsigned pk = prmt(H, F, 0x7632u);  // (H.hi, F.hi)
         unsigned sh = grp.shfl(pk, src);
         if (from_rv) sh = rv[u];
@@ -463,15 +470,31 @@ __global__ void __launch_bounds__(128) sw16_kernel(SwArgs a) {
 // pair here only then.  Under that bound no writer is ever more than P
 // entries ahead of its reader, so a ring of R >= P + 8 entries needs no
 // back-pressure.  Each writer publishes its progress after every chunk (ring
-// store, block fence, flag store); each reader spins on the flag with an
-// iteration limit, after which it records GMF_SWF_TIMEOUT and goes on.
+// store, then a release store of the flag); each reader polls the flag with
+// acquire loads and an iteration limit, after which it records
+// GMF_SWF_TIMEOUT and goes on.
 // Traceback words land at the same (global step, lane) positions as in the
 // one-warp layout, so the walk (warp 0, after a block barrier) is unchanged.
 // ---------------------------------------------------------------------------
 constexpr int COOP_WAIT_LIMIT = 1 << 22;  // spins (about 20 ns each) before a wait gives up
 
+// Progress flags between the warps of a CTA: the writer publishes with a
+// release store after its ring store, the reader polls with acquire loads;
+// neither waits for the thread's outstanding global loads or stores (a block
+// fence would).
+__device__ __forceinline__ int ld_acquire_cta(const int* p) {
+    int v;
+    asm volatile("ld.acquire.cta.shared.b32 %0, [%1];" : "=r"(v)
+                 : "r"((unsigned)__cvta_generic_to_shared(p)) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_cta(int* p, int v) {
+    asm volatile("st.release.cta.shared.b32 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(p)), "r"(v)
+                 : "memory");
+}
+
 template <int NW, bool TB, bool XD, int EM>
-__device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, volatile int* prog, int (*sbest)[3],
+__device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* prog, int (*sbest)[3],
                                uint32_t** sws) {
     constexpr int L = 32, V = 64;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -549,7 +572,7 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, volatile
                 if (s0 >= 1 && s0 < nstrips) {
                     const int e = t + 4 * L - (w == 0 ? P : 0);
                     int spins = 0;
-                    while (prog[wprev] < e + 4) {
+                    while (ld_acquire_cta(prog + wprev) < e + 4) {
                         // bounded: after the limit, or once any wait in the grid gave up
                         // (every later wait then ends within ~1k spins), record and go on
                         if (++spins > COOP_WAIT_LIMIT ||
@@ -559,7 +582,6 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, volatile
                         }
                         __nanosleep(20);
                     }
-                    __threadfence_block();
                     const uint4 r = *reinterpret_cast<const uint4*>(ring_in + (e & rmask));
                     rv[0] = r.x;
                     rv[1] = r.y;
@@ -574,13 +596,12 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, volatile
             chunk16<32, TB, EM>(c, K, grp, src, twin, tpv, lane == 0, rv, hk, pk);
             tpv = prmt(twin, tpv, 0x4344u);
             tw.advance(true);
+            if (lane == 31) {  // publish before the global store, so the release does not wait on it
+                *reinterpret_cast<uint4*>(ring_out + (t & rmask)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                st_release_cta(prog + w, t + 4);
+            }
             const int g0 = t + gofs;
             if (TB && kk >= 0 && (g0 >> 2) <= last_chunk) bits[(g0 >> 2) * L + lane] = c.acc;
-            if (lane == 31) {
-                *reinterpret_cast<uint4*>(ring_out + (t & rmask)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-                __threadfence_block();
-                prog[w] = t + 4;
-            }
             best16<XD>(lb, pos0, pos1, hk, g0, d);
             if (XD && kk >= 0) {
                 if (d == dW0 && row <= qlen) rowmax[row - 1] = make_int2(lo16(lb) - (int)K.Z, pos0);
@@ -655,7 +676,7 @@ template <int NW, bool TB, bool XD, int EM>
 __global__ void __launch_bounds__(32 * NW) sw16_coop_kernel(SwArgs a) {
     extern __shared__ uint4 coop_ring4[];
     uint32_t* rings = reinterpret_cast<uint32_t*>(coop_ring4);
-    __shared__ volatile int prog[NW];
+    __shared__ int prog[NW];
     __shared__ int sbest[NW][3];
     __shared__ uint32_t* sws;
     __shared__ int spair;
