@@ -73,6 +73,16 @@ class GmfSwResults(Structure):
     ]
 
 
+class GmfSwTuning(Structure):
+    _fields_ = [
+        ("l8_max_w", c_int32),
+        ("l16_max_w", c_int32),
+        ("coop_min_strips", c_int32 * 3),
+        ("warps_per_block", c_int32),
+        ("side_streams", c_int32),
+    ]
+
+
 class GmfChainParams(Structure):
     _fields_ = [
         ("max_lookback", c_int32),
@@ -128,6 +138,8 @@ _SIGNATURES = {
                               c_void_p, c_size_t, c_void_p]),
     "gmf_banded_sw_plain": (c_int, [POINTER(GmfPairs), POINTER(GmfSwParams), POINTER(GmfSwResults),
                                     c_void_p, c_size_t, c_void_p]),
+    "gmf_sw_get_tuning": (c_int, [POINTER(GmfSwTuning)]),
+    "gmf_sw_set_tuning": (c_int, [POINTER(GmfSwTuning)]),
     "gmf_chain_dp": (c_int, [c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32,
                              c_int32, c_void_p, c_int32, c_void_p, c_void_p, c_void_p]),
     "gmf_chain_sort": (c_int, [POINTER(GmfAnchorBatch), POINTER(GmfSortedAnchors), c_void_p,

@@ -25,9 +25,14 @@ inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? GMF_OK : GMF_E
 // Make the device that owns `stream` current for this thread (the library's
 // CUDA runtime is private, so its current device follows the caller's stream
 // rather than another runtime's state).  The legacy stream keeps the current
-// device.
+// device, and so does a stream that is being captured into a CUDA graph:
+// asking a capturing stream for its device invalidates the capture, so a
+// caller that captures selects the device first (gmf_set_device).
 inline int bind_stream_device(cudaStream_t stream) {
     if (stream == nullptr) return GMF_OK;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess) return GMF_ERR_CUDA;
+    if (cs != cudaStreamCaptureStatusNone) return GMF_OK;
     int dev = -1, cur = -1;
     if (cudaStreamGetDevice(stream, &dev) != cudaSuccess) return GMF_ERR_CUDA;
     if (cudaGetDevice(&cur) != cudaSuccess) return GMF_ERR_CUDA;

@@ -48,17 +48,18 @@ __host__ __device__ inline bool fits_int16(int qlen, int tlen, int match, int mi
 // 4)) and the pair has at least two strips per warp.  Each cooperative class
 // covers one period range [NW * 132, 2 * NW * 132) (the 8-warp class up to
 // COOP_PMAX); shorter pairs in those ranges take one warp.
-__host__ __device__ inline int sw_class(int qlen, int tlen, int hb, int match, int mism, int go, int ge) {
+__host__ __device__ inline int sw_class(int qlen, int tlen, int hb, int match, int mism, int go, int ge,
+                                        int l8w, int l16w, const int* cmin) {
     if (!fits_int16(qlen, tlen, match, mism, go, ge)) return CLS_I32;
     const int W = 2 * hb + 1;
-    if (W <= 61) return CLS_I16_L8;
-    if (W <= 125) return CLS_I16_L16;
+    if (W <= l8w) return CLS_I16_L8;
+    if (W <= l16w) return CLS_I16_L16;
     const int P = sw16_period(W, 32);
     const int strips = (qlen + 63) / 64;
     // each cooperative class holds one period range (its rings are sized for it)
-    if (P >= 8 * 132 && P <= COOP_PMAX) return strips >= 16 ? CLS_I16_C8 : CLS_I16_L32;
-    if (P >= 4 * 132 && P < 8 * 132) return strips >= 8 ? CLS_I16_C4 : CLS_I16_L32;
-    if (P >= 2 * 132 && P < 4 * 132) return strips >= 4 ? CLS_I16_C2 : CLS_I16_L32;
+    if (P >= 8 * 132 && P <= COOP_PMAX) return (cmin[2] > 0 && strips >= cmin[2]) ? CLS_I16_C8 : CLS_I16_L32;
+    if (P >= 4 * 132 && P < 8 * 132) return (cmin[1] > 0 && strips >= cmin[1]) ? CLS_I16_C4 : CLS_I16_L32;
+    if (P >= 2 * 132 && P < 4 * 132) return (cmin[0] > 0 && strips >= cmin[0]) ? CLS_I16_C2 : CLS_I16_L32;
     return CLS_I16_L32;
 }
 
@@ -71,7 +72,7 @@ __global__ void sw_classify_kernel(SwArgs a) {
             p = a.order ? a.order[idx] : idx;
             const int ql = (int)(a.q_off[p + 1] - a.q_off[p]);
             const int tl = (int)(a.t_off[p + 1] - a.t_off[p]);
-            cls = sw_class(ql, tl, a.hb[p], a.match, a.mismatch, a.gap_open, a.gap_extend);
+            cls = sw_class(ql, tl, a.hb[p], a.match, a.mismatch, a.gap_open, a.gap_extend, a.l8w, a.l16w, a.cmin);
         }
         const unsigned lt = (1u << lane) - 1u;
 #pragma unroll
@@ -108,8 +109,35 @@ struct SideStreams {
     bool ready;
 };
 constexpr int kMaxSideDevices = 64;
-std::mutex g_side_mu;  // guards creation and every fork/launch/join sequence
+std::mutex g_side_mu;  // guards side streams, tuning, and every fork/launch/join sequence
 SideStreams g_side[kMaxSideDevices];
+
+// Scheduling knobs per device (see gmf_sw_tuning).
+struct Tuning {
+    gmf_sw_tuning t;
+    bool set;
+};
+Tuning g_tuning[kMaxSideDevices];
+
+static gmf_sw_tuning default_tuning() {
+    gmf_sw_tuning t;
+    t.l8_max_w = 61;
+    t.l16_max_w = 125;
+    t.coop_min_strips[0] = 4;
+    t.coop_min_strips[1] = 8;
+    t.coop_min_strips[2] = 16;
+    t.warps_per_block = 4;
+    t.side_streams = 1;
+    return t;
+}
+
+static int current_tuning(gmf_sw_tuning* out) {  // caller holds g_side_mu
+    int dev = 0;
+    GMF_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxSideDevices) return GMF_ERR_LIMIT;
+    *out = g_tuning[dev].set ? g_tuning[dev].t : default_tuning();
+    return GMF_OK;
+}
 
 static int side_streams(SideStreams** out) {
     int dev = 0;
@@ -169,6 +197,11 @@ static void fill_args(SwArgs& a, const gmf_pairs* pairs, const gmf_sw_params* pa
     a.gap_open = params->gap_open;
     a.gap_extend = params->gap_extend;
     a.x_drop = params->x_drop;
+    a.l8w = 61;  // defaults; the batched form replaces them with the device's tuning
+    a.l16w = 125;
+    a.cmin[0] = 4;
+    a.cmin[1] = 8;
+    a.cmin[2] = 16;
     a.max_hb = pairs->max_half_band;
     const int pmax = max_penalty(params->mismatch_penalty, params->gap_open, params->gap_extend);
     a.zero16 = 4 * pmax + 2;
@@ -205,8 +238,8 @@ static int dev_info(DevInfo& di) {
 }
 
 // Warps per block that fit the per-warp shared memory.
-static int warps_per_block(size_t per_warp, const DevInfo& di) {
-    int wpb = 4;
+static int warps_per_block(size_t per_warp, const DevInfo& di, int cap = 4) {
+    int wpb = cap < 1 ? 1 : (cap > 4 ? 4 : cap);
     while (wpb > 1 && per_warp * wpb > (size_t)di.smem_optin) --wpb;
     return per_warp > (size_t)di.smem_optin ? 0 : wpb;
 }
@@ -273,6 +306,12 @@ extern "C" int gmf_banded_sw(const gmf_pairs* pairs, const gmf_sw_params* params
     const bool xd = params->x_drop > 0;
     const int em = e_mode_of(params);
     a.defer_walk = tb ? 1 : 0;
+    std::lock_guard<std::mutex> lock(g_side_mu);
+    gmf_sw_tuning tun;
+    GMF_TRY(current_tuning(&tun));
+    a.l8w = tun.l8_max_w;
+    a.l16w = tun.l16_max_w;
+    for (int i = 0; i < 3; ++i) a.cmin[i] = tun.coop_min_strips[i];
 
     const int cls_blocks = std::min((pairs->n_pairs + 255) / 256, di.sms * 4);
     sw_classify_kernel<<<cls_blocks, 256, 0, stream>>>(a);
@@ -280,13 +319,20 @@ extern "C" int gmf_banded_sw(const gmf_pairs* pairs, const gmf_sw_params* params
 
     const int Wmax = 2 * pairs->max_half_band + 1;
     const int Pmax = sw16_period(Wmax, 32);
-    // every class kernel goes to its own side stream, longest classes first
-    std::lock_guard<std::mutex> lock(g_side_mu);
+    // every class kernel goes to its own side stream (or, untuned-off, to the
+    // caller's stream), longest classes first
     SideStreams* ss = nullptr;
-    GMF_TRY(side_streams(&ss));
-    GMF_CUDA_TRY(cudaEventRecord(ss->fork, stream));
+    const bool fork = tun.side_streams != 0;
+    if (fork) {
+        GMF_TRY(side_streams(&ss));
+        GMF_CUDA_TRY(cudaEventRecord(ss->fork, stream));
+    }
     int used = 0;
     auto next_stream = [&](cudaStream_t* out) -> int {
+        if (!fork) {
+            *out = stream;
+            return GMF_OK;
+        }
         GMF_CUDA_TRY(cudaStreamWaitEvent(ss->s[used], ss->fork, 0));
         *out = ss->s[used++];
         return GMF_OK;
@@ -296,8 +342,9 @@ extern "C" int gmf_banded_sw(const gmf_pairs* pairs, const gmf_sw_params* params
     const int coop_cls[3] = {CLS_I16_C8, CLS_I16_C4, CLS_I16_C2};
     const int coop_pmin[3] = {8 * 132, 4 * 132, 2 * 132};
     const int coop_pcap[3] = {COOP_PMAX, 8 * 132 - 4, 4 * 132 - 4};
+    const int coop_knob[3] = {2, 1, 0};  // coop_min_strips index of C8, C4, C2
     for (int c = 0; c < 3; ++c) {
-        if (Pmax < coop_pmin[c]) continue;  // no pair can be in this class
+        if (Pmax < coop_pmin[c] || tun.coop_min_strips[coop_knob[c]] <= 0) continue;  // class empty
         SwArgs ac = a;
         ac.ring = ring_entries(std::min(Pmax, coop_pcap[c]) + 7);
         if ((size_t)sw16_coop_warps(coop_cls[c]) * ac.ring * 4 > (size_t)di.smem_optin) return GMF_ERR_LIMIT;
@@ -307,13 +354,13 @@ extern "C" int gmf_banded_sw(const gmf_pairs* pairs, const gmf_sw_params* params
     }
     // one-warp and shared-warp classes (a class only ever holds pairs up to
     // its own band limit), widest first
-    const int cls_wmax[3] = {std::min(Wmax, 61), std::min(Wmax, 125), Wmax};
+    const int cls_wmax[3] = {std::min(Wmax, tun.l8_max_w), std::min(Wmax, tun.l16_max_w), Wmax};
     const int lanes[3] = {8, 16, 32};
     for (int c = 2; c >= 0; --c) {
         const int L = lanes[c];
         SwArgs ac = a;
         ac.ring = ring_entries(std::max(3, sw16_period(cls_wmax[c], L) - 4 * L - 1));
-        const int wpb = warps_per_block((size_t)sw16_smem_per_warp(c, ac.ring), di);
+        const int wpb = warps_per_block((size_t)sw16_smem_per_warp(c, ac.ring), di, tun.warps_per_block);
         if (wpb == 0) return GMF_ERR_LIMIT;
         const int grid = di.sms * std::max(1, 16 / wpb);
         cudaStream_t s;
@@ -322,14 +369,14 @@ extern "C" int gmf_banded_sw(const gmf_pairs* pairs, const gmf_sw_params* params
     }
     SwArgs a32 = a;
     a32.ring = ring_entries(std::max(64, Wmax + 1) - 64);
-    const int wpb = warps_per_block((size_t)sw32_smem_per_warp(a32.ring), di);
+    const int wpb = warps_per_block((size_t)sw32_smem_per_warp(a32.ring), di, tun.warps_per_block);
     if (wpb == 0) return GMF_ERR_LIMIT;
     {
         cudaStream_t s;
         GMF_TRY(next_stream(&s));
         GMF_TRY(launch_sw32(a32, tb, xd, em, true, di.sms * std::max(1, 12 / wpb), wpb, s));
     }
-    for (int i = 0; i < used; ++i) {
+    for (int i = 0; fork && i < used; ++i) {
         GMF_CUDA_TRY(cudaEventRecord(ss->join[i], ss->s[i]));
         GMF_CUDA_TRY(cudaStreamWaitEvent(stream, ss->join[i], 0));
     }
@@ -352,4 +399,28 @@ extern "C" int gmf_banded_sw_plain(const gmf_pairs* pairs, const gmf_sw_params* 
     const int grid = (pairs->n_pairs + wpb - 1) / wpb;
     return launch_sw32(a, res->cigar != nullptr, params->x_drop > 0, e_mode_of(params), false, grid,
                        wpb, stream);
+}
+
+extern "C" int gmf_sw_get_tuning(gmf_sw_tuning* t) {
+    if (!t) return GMF_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(g_side_mu);
+    return current_tuning(t);
+}
+
+extern "C" int gmf_sw_set_tuning(const gmf_sw_tuning* t) {
+    if (!t) return GMF_ERR_INVALID_ARGUMENT;
+    const int wmax = 2 * GMF_MAX_HALF_BAND + 1;
+    if (t->l8_max_w < 0 || t->l8_max_w > wmax || t->l16_max_w < t->l8_max_w || t->l16_max_w > wmax)
+        return GMF_ERR_INVALID_ARGUMENT;
+    for (int i = 0; i < 3; ++i)
+        if (t->coop_min_strips[i] < 0 || t->coop_min_strips[i] > (1 << 24)) return GMF_ERR_INVALID_ARGUMENT;
+    if (t->warps_per_block < 1 || t->warps_per_block > 4 || (t->side_streams != 0 && t->side_streams != 1))
+        return GMF_ERR_INVALID_ARGUMENT;
+    int dev = 0;
+    GMF_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxSideDevices) return GMF_ERR_LIMIT;
+    std::lock_guard<std::mutex> lock(g_side_mu);
+    g_tuning[dev].t = *t;
+    g_tuning[dev].set = true;
+    return GMF_OK;
 }

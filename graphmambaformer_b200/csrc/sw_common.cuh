@@ -55,6 +55,8 @@ struct SwArgs {
     unsigned long long* cigar_used;
     int32_t* err;
     int32_t defer_walk;              // batched form: DP kernels leave the walk to sw_walk_kernel
+    int32_t l8w, l16w;               // classifier: widest bands of the 8- and 16-lane classes
+    int32_t cmin[3];                 // classifier: fewest strips of the 2-, 4-, 8-warp classes (0: off)
     unsigned long long* tb_base;     // per pair: first traceback word (pool offset)
     int32_t* tb_tag;                 // per pair: traceback layout (0 int32, L for 16x2), -1 none
 };

@@ -53,8 +53,9 @@ const char* gmf_status_string(int status);
 int gmf_version(void); /* major*10000 + minor*100 + patch */
 
 /* The library links its own CUDA runtime.  Calls given a non-NULL stream run
- * on that stream's device; calls on the legacy stream (NULL) run on the
- * device selected here (default 0). */
+ * on that stream's device; calls on the legacy stream (NULL), and calls made
+ * while their stream is being captured into a CUDA graph, run on the device
+ * selected here (default 0). */
 int gmf_set_device(int device);
 
 /* Limits enforced by the entry points (GMF_ERR_LIMIT beyond them). */
@@ -143,6 +144,27 @@ int gmf_banded_sw(const gmf_pairs* pairs, const gmf_sw_params* params,
 int gmf_banded_sw_plain(const gmf_pairs* pairs, const gmf_sw_params* params,
                         const gmf_sw_results* results, void* workspace, size_t workspace_bytes,
                         gmf_stream_t stream);
+
+/* Scheduling knobs of the batched form (per device, process-wide).  They
+ * decide which kernel shape aligns which pair and how the kernels overlap;
+ * results never depend on them.  graphmambaformer_b200.autotune times
+ * candidate settings on a sample of a workload and keeps the fastest.  No
+ * counterpart in the reference (its batched kernel has one fixed shape). */
+typedef struct {
+    int32_t l8_max_w;           /* bands W = 2*half_band+1 up to this take 8 lanes per pair */
+    int32_t l16_max_w;          /* ... up to this 16 lanes (>= l8_max_w); wider take a warp */
+    int32_t coop_min_strips[3]; /* 2-, 4-, 8-warp classes: fewest 64-row strips a pair needs
+                                   to be shared by that many warps; 0 disables the class */
+    int32_t warps_per_block;    /* one-warp classes: warps per CTA, 1..4 */
+    int32_t side_streams;       /* 1: class kernels overlap on side streams; 0: caller's stream */
+} gmf_sw_tuning;
+
+/* Current settings of the calling thread's current device (defaults: 61,
+ * 125, {4, 8, 16}, 4, 1). */
+int gmf_sw_get_tuning(gmf_sw_tuning* tuning);
+/* Replace them (GMF_ERR_INVALID_ARGUMENT for out-of-range values).  Takes
+ * effect for later gmf_banded_sw calls on that device. */
+int gmf_sw_set_tuning(const gmf_sw_tuning* tuning);
 
 /* ======================================================================== */
 /* Anchor chaining                                                          */
