@@ -138,6 +138,8 @@ _SIGNATURES = {
                               c_void_p, c_size_t, c_void_p]),
     "gmf_banded_sw_plain": (c_int, [POINTER(GmfPairs), POINTER(GmfSwParams), POINTER(GmfSwResults),
                                     c_void_p, c_size_t, c_void_p]),
+    "gmf_gather_segments": (c_int, [c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_void_p,
+                                    c_void_p, c_void_p]),
     "gmf_sw_get_tuning": (c_int, [POINTER(GmfSwTuning)]),
     "gmf_sw_set_tuning": (c_int, [POINTER(GmfSwTuning)]),
     "gmf_chain_dp": (c_int, [c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32,

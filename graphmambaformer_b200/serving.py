@@ -1,0 +1,384 @@
+"""Serving loop: chaining + extension for a stream of read requests.
+
+A request carries 1..64 reads (base codes) and their raw minimizer anchors
+(seeding happens on the client).  The server keeps the reference codes and
+the chaining penalty table resident on the device and, per batch of reads,
+runs the two stages of the reference's classical path
+(alignment/chaining.py L620-745 then alignment/extension.py L469-641):
+
+  1. ``gmf_chain_batch``: strand split + sort, DP, chain peeling, select;
+  2. the window and band of every kept chain (extension.py L489-509, on the
+     host from the chain records), then ``gmf_gather_segments`` builds the
+     queries (reads, reverse-complemented for strand -1) and the target
+     windows from the resident buffers on the device;
+  3. ``gmf_banded_sw`` (batched form) + CIGAR assembly with soft clips.
+
+Continuous batching: a dispatcher admits pending requests first-come
+first-served into a batch whenever one of the workers is free, as long as
+the batch's estimated device memory fits the working-memory budget (8 GB by
+default) next to the batches in flight.  Each worker runs its batches on its
+own CUDA stream, so a batch formed from requests that arrived while others
+were on the GPU overlaps with them on the device.  Per-read results do not
+depend on the batch (every stage is per read / per pair), so a request gets
+the same alignments alone or in any mix.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import queue
+import threading
+import time
+from concurrent.futures import Future
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _native
+from .chaining import LUTS, AnchorCSR, ChainingConfig, chain_params
+from .config import ExtensionConfig
+from .device import bind, require_cuda
+from .extension import SWResult, _result, longest_first, params_from_config
+from .session import _Buffers
+from .types import merge_cigar
+
+
+def estimate_bytes(read_lens: np.ndarray, n_anchors: int, cfg: ExtensionConfig, max_chains: int) -> int:
+    """Upper bound on a batch's device working memory: anchors with the
+    chaining workspace, and every possible chain's traceback bits."""
+    W = 2 * cfg.max_half_band + 1
+    cells = int(np.sum((np.asarray(read_lens, np.int64) + 2 * cfg.flank) * W)) * min(max_chains, 2)
+    return int(120 * n_anchors + cells // 2 + 64 * len(read_lens) + (1 << 20))
+
+
+class BatchAligner:
+    """The device pipeline for one batch of reads on one stream (grow-only
+    buffers, reused between batches)."""
+
+    def __init__(self, ref_d: torch.Tensor, device, chain_cfg: ChainingConfig, ext_cfg: ExtensionConfig,
+                 stream: Optional[torch.cuda.Stream] = None):
+        self.device = require_cuda(device)
+        self.ref_d = ref_d
+        self.ref_len = int(ref_d.numel())
+        self.ccfg, self.ecfg = chain_cfg, ext_cfg
+        self.cp = chain_params(chain_cfg)
+        self.sw = params_from_config(ext_cfg)
+        self.lut = LUTS.get(self.device, chain_cfg.max_gap, chain_cfg.gap_open, chain_cfg.gap_extend,
+                            chain_cfg.log_coeff)
+        self.stream = stream or torch.cuda.Stream(self.device)
+        self.buf = _Buffers(self.device)
+
+    def _call(self, name, *args):
+        _native.check(name, getattr(_native.lib(), name)(*args))
+
+    def align(self, reads: Sequence[np.ndarray], anchors) -> list:
+        """Per read, the list of its chains' ExtensionResults (in select
+        order), exactly as AffineChainer.chain + ExtensionEngine.extend_chains
+        give them."""
+        a = AnchorCSR.of(anchors)
+        R = len(reads)
+        if R != len(a):
+            raise ValueError("one anchor set per read is required")
+        if R == 0:
+            return []
+        s, up, db = self.stream, self.buf.upload, self.buf.device_buf
+        sp = int(s.cuda_stream)
+        bind(self.device, sp)
+        rl = np.array([len(x) for x in reads], np.int64)
+        roff = np.zeros(R + 1, np.int64)
+        np.cumsum(rl, out=roff[1:])
+        codes = np.concatenate(reads).astype(np.int8) if roff[-1] else np.zeros(1, np.int8)
+        reads_d = up("reads", codes, s)
+        A = int(a.read_off[-1])
+        if np.diff(a.read_off).max(initial=0) > _native.MAX_READ_ANCHORS:
+            raise ValueError(f"a read has more than {_native.MAX_READ_ANCHORS} anchors")
+        pad = lambda x, dt: x if len(x) else np.zeros(1, dt)  # noqa: E731
+        ro = up("ro", a.read_off, s)
+        rp = up("rp", pad(a.read_pos, np.int32), s)
+        fp = up("fp", pad(a.ref_pos, np.int32), s)
+        ln = up("ln", pad(a.length, np.int32), s)
+        st = up("st", pad(a.strand, np.int8), s)
+        mc = self.cp.max_chains
+        o = dict(n=db("n", R, torch.int32), score=db("score", R * mc, torch.float64),
+                 strand=db("strand", R * mc, torch.int32), span=db("span", 4 * R * mc, torch.int32),
+                 prim=db("prim", R * mc, torch.int32), nmem=db("nmem", R * mc, torch.int32),
+                 mem=db("mem", max(A, 1), torch.int32))
+        need = int(_native.lib().gmf_chain_workspace_bytes(R, A))
+        ws = db("cws", need, torch.uint8)
+        batch_c = _native.GmfAnchorBatch(R, ro.data_ptr(), rp.data_ptr(), fp.data_ptr(), ln.data_ptr(), st.data_ptr())
+        res_c = _native.GmfChainResults(o["n"].data_ptr(), o["score"].data_ptr(), o["strand"].data_ptr(),
+                                        o["span"].data_ptr(), o["prim"].data_ptr(), o["nmem"].data_ptr(),
+                                        o["mem"].data_ptr())
+        self._call("gmf_chain_batch", ctypes.byref(batch_c), ctypes.byref(self.cp),
+                   ctypes.c_void_p(self.lut.data_ptr()), self.lut.numel(), None, None, None, ctypes.byref(res_c),
+                   ctypes.c_void_p(ws.data_ptr()), need, ctypes.c_void_p(sp))
+        dl = self.buf.download
+        h = {k: dl("h_" + k, o[k], n, s) for k, n in
+             (("n", R), ("strand", R * mc), ("span", 4 * R * mc), ("nmem", R * mc), ("mem", A))}
+        s.synchronize()
+        n_ch = h["n"][:R].numpy()
+        strand = h["strand"][: R * mc].numpy().reshape(R, mc)
+        span = h["span"][: 4 * R * mc].numpy().reshape(R, mc, 4)
+        nmem = h["nmem"][: R * mc].numpy().reshape(R, mc)
+        mem = h["mem"][:A].numpy()
+
+        # ---- windows (extension.py L489-509), one pair per kept chain ----
+        cr, ck = np.nonzero(np.arange(mc)[None, :] < n_ch[:, None])  # (read, slot) of every chain
+        C = len(cr)
+        results: list = [[] for _ in range(R)]
+        if C == 0:
+            return results
+        m = nmem[cr, ck].astype(np.int64)
+        # members of chain (r, k) start after the members of slots < k of read r
+        first = a.read_off[cr] + (np.cumsum(nmem, axis=1) - nmem)[cr, ck]
+        seg = np.zeros(C + 1, np.int64)
+        np.cumsum(m, out=seg[1:])
+        flat = np.repeat(first - seg[:-1], m) + np.arange(int(seg[-1]), dtype=np.int64)
+        gidx = a.read_off[np.repeat(cr, m)] + mem[flat]
+        dg = a.ref_pos[gidx].astype(np.int64) - a.read_pos[gidx].astype(np.int64)
+        nz = m > 0
+        spread = np.zeros(C, np.int64)
+        if nz.any():
+            starts = seg[:-1][nz]
+            spread[nz] = np.maximum.reduceat(dg, starts) - np.minimum.reduceat(dg, starts)
+        cfg = self.ecfg
+        diag = span[cr, ck, 2].astype(np.int64) - span[cr, ck, 0].astype(np.int64)
+        rlen = rl[cr]
+        wstart = np.maximum(0, diag - cfg.flank)
+        wend = np.minimum(self.ref_len, diag + rlen + cfg.flank)
+        wend = np.where(wend - wstart > cfg.max_window, wstart + cfg.max_window, wend)
+        wlen = np.maximum(wend - wstart, 0)
+        hb = np.minimum(cfg.half_band + spread, cfg.max_half_band).astype(np.int32)
+        boff = (diag - wstart).astype(np.int32)
+        qoff = np.zeros(C + 1, np.int64)
+        np.cumsum(rlen, out=qoff[1:])
+        toff = np.zeros(C + 1, np.int64)
+        np.cumsum(wlen, out=toff[1:])
+
+        # ---- queries and targets gathered from the resident buffers ----
+        qd = db("q", max(int(qoff[-1]), 1), torch.int8)
+        td = db("t", max(int(toff[-1]), 1), torch.int8)
+        qs_d, ql_d = up("qs", roff[cr], s), up("ql", rlen.astype(np.int32), s)
+        rc_d, qo_d = up("rc", (strand[cr, ck] < 0).astype(np.int8), s), up("qo", qoff, s)
+        ts_d, tl_d, to_d = up("ts", wstart, s), up("tl", wlen.astype(np.int32), s), up("to", toff, s)
+        self._call("gmf_gather_segments", ctypes.c_void_p(reads_d.data_ptr()), int(roff[-1]), C,
+                   ctypes.c_void_p(qs_d.data_ptr()), ctypes.c_void_p(ql_d.data_ptr()),
+                   ctypes.c_void_p(rc_d.data_ptr()), ctypes.c_void_p(qd.data_ptr()),
+                   ctypes.c_void_p(qo_d.data_ptr()), ctypes.c_void_p(sp))
+        self._call("gmf_gather_segments", ctypes.c_void_p(self.ref_d.data_ptr()), self.ref_len, C,
+                   ctypes.c_void_p(ts_d.data_ptr()), ctypes.c_void_p(tl_d.data_ptr()), None,
+                   ctypes.c_void_p(td.data_ptr()), ctypes.c_void_p(to_d.data_ptr()), ctypes.c_void_p(sp))
+
+        # ---- banded SW + traceback (batched form) ----
+        hb_d, bo_d = up("hb", hb, s), up("bo", boff, s)
+        ord_d = up("ord", longest_first(rlen.astype(np.int32), hb), s)
+        out = dict(score=db("sc", C, torch.int32), qe=db("qe", C, torch.int32), te=db("te", C, torch.int32),
+                   qs=db("qs2", C, torch.int32), ts=db("ts2", C, torch.int32), clen=db("cl", C, torch.int32),
+                   counts=db("cn", 4 * C, torch.int32), cstart=db("cs", C, torch.int64),
+                   used=db("used", 1, torch.int64), err=db("err", 1, torch.int32))
+        cap = int(qoff[-1] + toff[-1] + C)
+        cigar = db("cigar", cap, torch.int32)
+        need = int(_native.lib().gmf_banded_sw_workspace_bytes(
+            C, rlen.astype(np.int32).ctypes.data_as(ctypes.c_void_p),
+            wlen.astype(np.int32).ctypes.data_as(ctypes.c_void_p), hb.ctypes.data_as(ctypes.c_void_p), 1))
+        sws = db("sws", need, torch.uint8)
+        pairs_c = _native.GmfPairs(C, qd.data_ptr(), qo_d.data_ptr(), td.data_ptr(), to_d.data_ptr(), hb_d.data_ptr(),
+                                   bo_d.data_ptr(), ord_d.data_ptr(), int(hb.max()))
+        sres = _native.GmfSwResults(out["score"].data_ptr(), out["qe"].data_ptr(), out["te"].data_ptr(),
+                                    out["qs"].data_ptr(), out["ts"].data_ptr(), out["counts"].data_ptr(),
+                                    cigar.data_ptr(), cap, out["cstart"].data_ptr(), out["clen"].data_ptr(),
+                                    out["used"].data_ptr(), out["err"].data_ptr())
+        self._call("gmf_banded_sw", ctypes.byref(pairs_c), ctypes.byref(self.sw), ctypes.byref(sres),
+                   ctypes.c_void_p(sws.data_ptr()), need, ctypes.c_void_p(sp))
+        hh = {k: dl("h2_" + k, out[k], n, s) for k, n in
+              (("score", C), ("qe", C), ("te", C), ("qs", C), ("ts", C), ("clen", C), ("counts", 4 * C),
+               ("cstart", C), ("used", 1), ("err", 1))}
+        s.synchronize()
+        used = int(hh["used"][0])
+        words = dl("h2_cigar", cigar, used, s)
+        s.synchronize()
+        res = SWResult(hh["score"][:C].numpy(), hh["qe"][:C].numpy(), hh["te"][:C].numpy(),
+                       hh["qs"][:C].numpy(), hh["ts"][:C].numpy(), hh["counts"][: 4 * C].numpy().reshape(C, 4),
+                       words[:used].numpy().view(np.uint32), hh["cstart"][:C].numpy(), hh["clen"][:C].numpy(),
+                       int(hh["err"][0]))
+        if res.error_flags:
+            raise RuntimeError(f"gmf_banded_sw reported error flags {res.error_flags}")
+        for c in range(C):  # ExtensionEngine._finish: window start and soft clips
+            ext = _result(res, c)
+            ext.ref_start += int(wstart[c])
+            ext.ref_end += int(wstart[c])
+            ext.cigar = merge_cigar([("S", ext.read_start)] + ext.cigar + [("S", int(rlen[c]) - ext.read_end)])
+            results[int(cr[c])].append(ext)
+        return results
+
+
+@dataclass
+class Request:
+    rid: int
+    reads: list
+    anchors: object
+    nbytes: int
+    arrival: float
+    future: Future = field(default_factory=Future)
+    done: float = 0.0
+
+
+class AlignServer:
+    """Continuous-batching server of chaining + extension requests."""
+
+    def __init__(self, ref_codes: np.ndarray, device=None, chain_cfg: Optional[ChainingConfig] = None,
+                 ext_cfg: Optional[ExtensionConfig] = None, budget_bytes: int = 8 << 30,
+                 max_batch_reads: int = 512, workers: int = 2):
+        self.device = require_cuda(device)
+        self.ccfg = chain_cfg or ChainingConfig()
+        self.ecfg = ext_cfg or ExtensionConfig()
+        self.budget = int(budget_bytes)
+        self.max_batch_reads = int(max_batch_reads)
+        torch.cuda.set_device(self.device)
+        self.ref_d = torch.from_numpy(np.ascontiguousarray(ref_codes, np.int8)).to(self.device)  # resident
+        self.workers = [BatchAligner(self.ref_d, self.device, self.ccfg, self.ecfg) for _ in range(workers)]
+        self.free: "queue.Queue[BatchAligner]" = queue.Queue()
+        for w in self.workers:
+            self.free.put(w)
+        self.pending: "queue.Queue[Request]" = queue.Queue()
+        self.in_flight_bytes = 0
+        self.lock = threading.Lock()
+        self.completed: list = []
+        self.batches = 0
+        self._next = 0
+        self._stop = threading.Event()
+        self._dispatcher = threading.Thread(target=self._dispatch, daemon=True)
+        self._threads: list = []
+
+    # -- client side -------------------------------------------------------------
+    def submit(self, reads: Sequence[np.ndarray], anchors) -> Future:
+        a = AnchorCSR.of(anchors)
+        nb = estimate_bytes(np.array([len(x) for x in reads], np.int64), int(a.read_off[-1]), self.ecfg,
+                            self.ccfg.max_chains)
+        if nb > self.budget:
+            raise ValueError("request larger than the working-memory budget")
+        with self.lock:
+            rid = self._next
+            self._next += 1
+        req = Request(rid, list(reads), a, nb, time.perf_counter())
+        self.pending.put(req)
+        return req.future
+
+    def start(self) -> "AlignServer":
+        self._dispatcher.start()
+        return self
+
+    def stop(self) -> None:
+        self._stop.set()
+        self._dispatcher.join(timeout=30)
+        for t in self._threads:
+            t.join(timeout=60)
+
+    # -- server side -------------------------------------------------------------
+    def _dispatch(self) -> None:
+        carry: Optional[Request] = None
+        while not self._stop.is_set():
+            try:
+                w = self.free.get(timeout=0.05)
+            except queue.Empty:
+                continue
+            batch, nbytes, nreads = [], 0, 0
+            deadline = time.perf_counter() + 0.5
+            while True:
+                if carry is None:
+                    try:
+                        carry = self.pending.get(timeout=0.001 if batch else 0.05)
+                    except queue.Empty:
+                        if batch or self._stop.is_set() or time.perf_counter() > deadline:
+                            break
+                        continue
+                with self.lock:
+                    fits = self.in_flight_bytes + nbytes + carry.nbytes <= self.budget
+                if batch and (not fits or nreads + len(carry.reads) > self.max_batch_reads):
+                    break
+                if not batch and not fits:  # wait for memory to free up
+                    time.sleep(0.001)
+                    continue
+                batch.append(carry)
+                nbytes += carry.nbytes
+                nreads += len(carry.reads)
+                carry = None
+            if not batch:
+                self.free.put(w)
+                continue
+            with self.lock:
+                self.in_flight_bytes += nbytes
+            t = threading.Thread(target=self._run, args=(w, batch, nbytes), daemon=True)
+            self._threads = [x for x in self._threads if x.is_alive()] + [t]
+            t.start()
+
+    def _run(self, w: BatchAligner, batch: list, nbytes: int) -> None:
+        try:
+            reads = [r for req in batch for r in req.reads]
+            anchors = AnchorCSR.from_sets(
+                [_ReadAnchors(req.anchors, i) for req in batch for i in range(len(req.reads))])
+            res = w.align(reads, anchors)
+            pos = 0
+            now = time.perf_counter()
+            for req in batch:
+                out = res[pos: pos + len(req.reads)]
+                pos += len(req.reads)
+                req.done = now
+                req.future.set_result(out)
+            with self.lock:
+                self.completed.extend(batch)
+                self.batches += 1
+        except BaseException as e:  # surface the error to every request of the batch
+            for req in batch:
+                if not req.future.done():
+                    req.future.set_exception(e)
+        finally:
+            with self.lock:
+                self.in_flight_bytes -= nbytes
+            self.free.put(w)
+
+    def latency_stats(self) -> dict:
+        with self.lock:
+            lat = np.array([(r.done - r.arrival) * 1e3 for r in self.completed])
+            nreads = sum(len(r.reads) for r in self.completed)
+        if not len(lat):
+            return {"requests": 0}
+        return {"requests": int(len(lat)), "reads": int(nreads), "batches": self.batches,
+                "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                "mean_ms": float(lat.mean()), "max_ms": float(lat.max())}
+
+
+class _ReadAnchors:
+    """Read i of an AnchorCSR viewed as an AnchorSet-like object (for
+    AnchorCSR.from_sets)."""
+
+    def __init__(self, a: AnchorCSR, i: int):
+        s, e = int(a.read_off[i]), int(a.read_off[i + 1])
+        self.read_pos, self.ref_pos = a.read_pos[s:e], a.ref_pos[s:e]
+        self.length, self.strand = a.length[s:e], a.strand[s:e]
+
+    def __len__(self) -> int:
+        return len(self.read_pos)
+
+
+def serve_stream(server: AlignServer, pool, requests: list, time_scale: float = 1.0) -> dict:
+    """Replay a request stream (list of (arrival seconds, read indices)
+    into ``pool``) against a started server, then wait for every result.
+    Returns latency / throughput figures."""
+    t0 = time.perf_counter()
+    futs = []
+    for arr, idx in requests:
+        wait = t0 + arr * time_scale - time.perf_counter()
+        if wait > 0:
+            time.sleep(wait)
+        reads, anchors = pool.take(idx)
+        futs.append(server.submit(reads, anchors))
+    for f in futs:
+        f.result(timeout=600)
+    wall = time.perf_counter() - t0
+    st = server.latency_stats()
+    st["wall_s"] = wall
+    st["reads_per_s"] = st.get("reads", 0) / wall if wall > 0 else 0.0
+    return st

@@ -408,3 +408,76 @@ def chaining_reads_hifi(n_reads: int = 5_000, seed: int = 2, ref_len: int = 10_0
         batch.meta["reads"] = reads
         batch.meta["ref"] = ref
     return batch
+
+
+# --------------------------------------------------------------------------- #
+# Serving workload: reads of the mixed profile with their anchors, requests
+# arriving as a Poisson stream
+# --------------------------------------------------------------------------- #
+@dataclass
+class ReadPool:
+    """Simulated reads (codes, as sequenced) of one reference, with their raw
+    minimizer anchors in both orientations (client-side seeding)."""
+
+    ref: np.ndarray
+    reads: list
+    anchors: AnchorBatch
+    profile: np.ndarray  # int8 per read (0 illumina, 1 hifi, 2 ont)
+
+    def __len__(self) -> int:
+        return len(self.reads)
+
+    def take(self, idx) -> tuple:
+        idx = np.asarray(idx, dtype=np.int64)
+        return [self.reads[int(i)] for i in idx], self.anchors.subset(idx)
+
+
+def mixed_read_pool(n_reads: int = 4000, seed: int = 4, ref_len: int = 10_000_000, min_len: int = 150,
+                    max_len: int = 20_000, log_mean: float = 7.0, log_sigma: float = 1.2, k: int = 15,
+                    w: int = 10) -> ReadPool:
+    """Reads with the length and error mix of the mixed extension workload
+    (log-normal lengths, one third each Illumina-like, HiFi-like and
+    ONT-like), random strand and position, seeded by (k, w) minimizers."""
+    rng = np.random.default_rng(seed)
+    ref = random_reference(ref_len, rng)
+    sketch = MinimizerSketch(ref, k=k, w=w)
+    lens = np.clip(rng.lognormal(log_mean, log_sigma, size=n_reads), min_len, max_len).astype(np.int64)
+    prof_id = rng.integers(0, 3, size=n_reads).astype(np.int8)
+    strands = np.where(rng.random(n_reads) < 0.5, 1, -1)
+    starts = rng.integers(0, ref_len - max_len - 1, size=n_reads)
+    profs = (ILLUMINA, HIFI, ONT)
+    reads, rp, fp, ln, st, counts = [], [], [], [], [], []
+    for r in range(n_reads):
+        tmpl = ref[starts[r]: starts[r] + lens[r]]
+        if strands[r] < 0:
+            tmpl = reverse_complement(tmpl)
+        read = apply_errors(tmpl, profs[prof_id[r]], rng)
+        reads.append(read)
+        n = 0
+        for s, codes in ((1, read), (-1, reverse_complement(read))):
+            a, b = sketch.query(codes)
+            rp.append(a)
+            fp.append(b)
+            ln.append(np.full(len(a), k, np.int64))
+            st.append(np.full(len(a), s, np.int8))
+            n += len(a)
+        counts.append(n)
+    off = np.zeros(n_reads + 1, dtype=np.int64)
+    np.cumsum(counts, out=off[1:])
+    batch = AnchorBatch(off, np.concatenate(rp).astype(np.int32), np.concatenate(fp).astype(np.int32),
+                        np.concatenate(ln).astype(np.int32), np.concatenate(st).astype(np.int8),
+                        np.array([len(x) for x in reads], np.int64),
+                        dict(workload="mixed_read_pool", seed=seed, ref_len=ref_len))
+    return ReadPool(ref, reads, batch, prof_id)
+
+
+def poisson_requests(n_requests: int, reads_per_s: float, pool_size: int, seed: int = 5, min_reads: int = 1,
+                     max_reads: int = 64) -> list:
+    """Requests of ``min_reads``..``max_reads`` reads (uniform) drawn from a
+    pool, arriving as a Poisson process whose rate gives ``reads_per_s``
+    reads per second on average: a list of (arrival seconds, read indices)."""
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(min_reads, max_reads + 1, size=n_requests)
+    rate = reads_per_s / ((min_reads + max_reads) / 2.0)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_requests))
+    return [(float(arrivals[i]), rng.integers(0, pool_size, size=int(sizes[i]))) for i in range(n_requests)]

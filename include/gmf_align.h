@@ -145,6 +145,17 @@ int gmf_banded_sw_plain(const gmf_pairs* pairs, const gmf_sw_params* params,
                         const gmf_sw_results* results, void* workspace, size_t workspace_bytes,
                         gmf_stream_t stream);
 
+/* Concatenates n segments of base codes: segment i is src[start[i] ..
+ * start[i] + len[i]) -- reversed and complemented (1<->4, 2<->3, other codes
+ * kept) when rc is non-NULL and rc[i] != 0 -- written to dst[dst_off[i] ..].
+ * Positions outside [0, src_len) read as -1 (padding).  Builds the query and
+ * target codes of an extension batch from a resident reference and resident
+ * reads.  Replaces the host-side window slicing of alignment/extension.py
+ * L489-509 (_window) and seeding.py L64-81 (reverse_complement_codes). */
+int gmf_gather_segments(const int8_t* src, int64_t src_len, int32_t n, const int64_t* start,
+                        const int32_t* len, const int8_t* rc, int8_t* dst, const int64_t* dst_off,
+                        gmf_stream_t stream);
+
 /* Scheduling knobs of the batched form (per device, process-wide).  They
  * decide which kernel shape aligns which pair and how the kernels overlap;
  * results never depend on them.  graphmambaformer_b200.autotune times
