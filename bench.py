@@ -56,6 +56,10 @@ def parse():
     p.add_argument("--chain-reads", type=int, default=5_000)
     p.add_argument("--no-chain", action="store_true")
     p.add_argument("--no-150bp", action="store_true")
+    p.add_argument("--no-serve", action="store_true")
+    p.add_argument("--no-autotune", action="store_true")
+    p.add_argument("--serve-load", type=float, default=20_000.0, help="offered load of the serving leg, reads/s")
+    p.add_argument("--serve-requests", type=int, default=600)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile-case", action="store_true",
                    help="small single-GPU case for ncu captures (no timing JSON)")
@@ -325,6 +329,19 @@ def run_b200(args):
                     e2e_ms=e, rank_ms=float(np.mean(b_ms)), sess=sess,
                     launches=launches_per_call(dp.max_half_band, True))
 
+    # ---- autotuned scheduling of the batched form (on a 10% sample of the
+    # headline workload; outside every timed region) ----
+    tuning = None
+    if not args.no_autotune:
+        from graphmambaformer_b200 import autotune
+
+        ps_s, params_s, _ = sw_workload(args.workload, args.pairs, seed=1 + 1000 * rank)
+        rng = np.random.default_rng(99)
+        sample = ps_s.subset(np.sort(rng.choice(len(ps_s), size=max(1, len(ps_s) // 10), replace=False)))
+        rep = autotune.autotune_sw(sample, extension.sw_params(*params_s), device, reps=2, passes=1)
+        tuning = dict(rep.as_dict(), sample_pairs=len(sample))
+        del ps_s, sample
+
     uuid = str(getattr(torch.cuda.get_device_properties(device), "uuid", ""))
     sampler = ClockSampler(uuid)
     head = sw_leg(args.workload, args.pairs, 1 + 1000 * rank, clocks=sampler)
@@ -369,6 +386,11 @@ def run_b200(args):
                     "h2d_bytes_per_step": csess.h2d_bytes, "d2h_bytes_per_step": csess.d2h_bytes},
         }
 
+    # ---- serving loop: Poisson requests of 1-64 mixed-profile reads ----
+    serve = None
+    if not args.no_serve:
+        serve = serve_leg(args, device, seed=7 + 1000 * rank)
+
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -402,7 +424,8 @@ def run_b200(args):
         "data": "synthetic (seeded, reference simulator error model)",
         "config": dict(head["desc"], parallelism=f"replicas x{world}", l2="flushed between timed steps",
                        traceback="on (CIGAR per pair)",
-                       form="batched: device classifier, class kernels on side streams, deferred walk"),
+                       form="batched: device classifier, class kernels on side streams, deferred walk",
+                       tuning=tuning or "defaults"),
         "e2e": {"value": head["total"] / (head["e2e_ms"] * 1e-3) / 1e9, "unit": "GCUPS",
                 "ms_per_step": head["e2e_ms"], "h2d_bytes_per_step": head["sess"].h2d_bytes,
                 "d2h_bytes_per_step": head["sess"].d2h_bytes,
@@ -434,9 +457,38 @@ def run_b200(args):
             "gpu_launches_per_step": small["launches"]}
     if chain:
         line["chain"] = chain
+    if serve:
+        line["serving"] = serve
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ps, head["params"])
     return line
+
+
+def serve_leg(args, device, seed: int) -> dict:
+    """p50/p99 request latency and throughput of the serving loop at a fixed
+    offered load: Poisson arrivals of requests of 1-64 reads drawn from a
+    pool of mixed-profile reads (lengths 150 bp - 20 kb) on a 10 Mb
+    reference kept on the device, 8 GB working-memory budget."""
+    from graphmambaformer_b200 import synth
+    from graphmambaformer_b200.serving import AlignServer, serve_stream
+
+    pool = synth.mixed_read_pool(n_reads=2000, seed=seed, ref_len=10_000_000)
+    srv = AlignServer(pool.ref, device, budget_bytes=8 << 30, workers=2, max_batch_reads=512).start()
+    try:
+        warm = synth.poisson_requests(40, args.serve_load, len(pool), seed=seed + 1)
+        serve_stream(srv, pool, warm)
+        srv.completed.clear()
+        srv.batches = 0
+        reqs = synth.poisson_requests(args.serve_requests, args.serve_load, len(pool), seed=seed + 2)
+        st = serve_stream(srv, pool, reqs)
+    finally:
+        srv.stop()
+    return {"offered_reads_per_s": args.serve_load, "achieved_reads_per_s": st["reads_per_s"],
+            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+            "requests": st["requests"], "reads": st["reads"], "batches": st["batches"],
+            "config": {"reference": "10 Mb uniform, resident on the device", "requests": "1-64 reads, Poisson",
+                       "reads": "pool of 2,000 mixed-profile reads (150 bp - 20 kb), client-side minimizers",
+                       "budget": "8 GB", "workers": 2, "max_batch_reads": 512}}
 
 
 # --------------------------------------------------------------------------- #
