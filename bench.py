@@ -58,6 +58,8 @@ def parse():
     p.add_argument("--no-150bp", action="store_true")
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--no-autotune", action="store_true")
+    p.add_argument("--long-reads", type=int, default=200,
+                   help="reads of the long-read stress leg (2,000 = the full configuration; 0 skips it)")
     p.add_argument("--serve-load", type=float, default=20_000.0, help="offered load of the serving leg, reads/s")
     p.add_argument("--serve-requests", type=int, default=600)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -386,6 +388,11 @@ def run_b200(args):
                     "h2d_bytes_per_step": csess.h2d_bytes, "d2h_bytes_per_step": csess.d2h_bytes},
         }
 
+    # ---- long-read stress: 50-100 kb ONT-like reads, h = 200 chaining, gap SW ----
+    longr = None
+    if args.long_reads > 0:
+        longr = long_read_leg(args, device, stream, flush, seed=6 + 1000 * rank, warm=warm)
+
     # ---- serving loop: Poisson requests of 1-64 mixed-profile reads ----
     serve = None
     if not args.no_serve:
@@ -459,9 +466,71 @@ def run_b200(args):
         line["chain"] = chain
     if serve:
         line["serving"] = serve
+    if longr:
+        line["long_reads"] = longr
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ps, head["params"])
     return line
+
+
+def long_read_leg(args, device, stream, flush, seed: int, warm: int) -> dict:
+    """Long-read stress: ONT-like reads of 50-100 kb on a 50 Mb reference,
+    chained with a 200-anchor window; banded SW over the primary chain's gaps
+    (graphmambaformer_b200.longreads).  Device times of the chaining call and
+    of the gap-SW call, each the mean of the timed steps."""
+    import torch
+
+    from graphmambaformer_b200 import chaining, longreads, synth
+    from graphmambaformer_b200.config import ChainingConfig
+
+    pool = synth.long_reads_ont(n_reads=args.long_reads, seed=seed)
+    al = longreads.LongReadAligner(torch.from_numpy(pool.ref).to(device), device)
+    prim, _ = al.primary_chains(pool.reads, pool.anchors)
+    seg = al.segments(pool.reads, prim)
+    cfg = ChainingConfig(max_lookback=200)
+    da = chaining.upload_anchors(pool.anchors, device)
+    cout = chaining.ChainOutputs.allocate(da, cfg.max_chains)
+
+    def cstep():
+        chaining.launch_chain_batch(da, cfg, out=cout, stream=stream)
+
+    for _ in range(warm):
+        cstep()
+    torch.cuda.synchronize(device)
+    c_ms = float(np.mean(time_device(cstep, args.steps, stream, flush)))
+    # gap SW: the segments as a resident pair batch
+    from graphmambaformer_b200 import extension
+
+    qs, ts = [], []
+    for i in range(len(seg)):
+        read = pool.reads[int(seg.read[i])]
+        frame = read if seg.strand[i] > 0 else synth.reverse_complement(read)
+        qs.append(frame[seg.q_start[i]: seg.q_start[i] + seg.q_len[i]])
+        ts.append(pool.ref[seg.t_start[i]: seg.t_start[i] + seg.t_len[i]])
+    ps = synth.PairSet.from_lists(qs, ts, seg.half_band, seg.band_offset)
+    dp = extension.upload_pairs(ps, device)
+    sw_p = extension.params_from_config(al.ecfg)
+    out = extension.SWOutputs.allocate(dp, True)
+    ws = torch.empty(extension.workspace_bytes(dp, True), dtype=torch.uint8, device=device)
+
+    def sstep():
+        extension.launch_banded_sw(dp, sw_p, True, out=out, workspace=ws, stream=stream)
+
+    for _ in range(warm):
+        sstep()
+    torch.cuda.synchronize(device)
+    s_ms = float(np.mean(time_device(sstep, args.steps, stream, flush)))
+    cells = ps.cells()
+    return {"reads": len(pool), "anchors": pool.anchors.n_anchors,
+            "chain": {"value": pool.anchors.n_anchors / (c_ms * 1e-3), "unit": "anchors/s", "ms_per_step": c_ms,
+                      "lookback": 200},
+            "gap_sw": {"value": cells / (s_ms * 1e-3) / 1e9, "unit": "GCUPS", "ms_per_step": s_ms,
+                       "segments": len(seg), "cells": cells, "max_half_band": int(seg.half_band.max()),
+                       "scoring": "extension defaults 2/4/6/2, x-drop 600"},
+            "config": {"reference": "50 Mb uniform", "reads": "ONT-like 5% error (60% indels), 50-100 kb",
+                       "segmentation": "primary chain cut at anchors >= 1 kb apart; band clip(32 + |drift| + "
+                                       "len/50, 32, 2000)",
+                       "sample": f"{len(pool)} of the configuration's 2,000 reads" if len(pool) < 2000 else "full"}}
 
 
 def serve_leg(args, device, seed: int) -> dict:
