@@ -372,11 +372,22 @@ __global__ void __launch_bounds__(256) chain_peel_kernel(PeelArgs a) {
         __syncthreads();
         block_bitonic(key, idx, np2);
         __syncthreads();
+        const int c_first = n_cand;  // chains found in earlier segments
+        // the serial walk reads predecessors and claimed flags at every step:
+        // when the strand sorted in shared memory, the dead sort keys hold them
+        const bool in_smem = np2 <= a.smem_elems;
+        int8_t* claimed = in_smem ? reinterpret_cast<int8_t*>(reinterpret_cast<int32_t*>(key) + np2)
+                                  : a.claimed + a0;
+        const int32_t* par = a.parent + a0 + s0;
+        if (in_smem) {
+            int32_t* par_s = reinterpret_cast<int32_t*>(key);  // 4*np2 + np2 bytes <= 8*np2
+            for (int x = threadIdx.x; x < n; x += blockDim.x) par_s[x] = par[x];
+            par = par_s;
+        }
+        for (int x = threadIdx.x; x < n; x += blockDim.x) claimed[x] = 0;
+        __syncthreads();
         if (threadIdx.x == 0) {
-            int8_t* claimed = a.claimed + a0;
-            for (int x = 0; x < n; ++x) claimed[x] = 0;
             const double* f = a.f + a0 + s0;
-            const int32_t* par = a.parent + a0 + s0;
             for (int k = 0; k < n; ++k) {
                 const int i = idx[k];
                 if (claimed[i]) continue;
@@ -391,22 +402,37 @@ __global__ void __launch_bounds__(256) chain_peel_kernel(PeelArgs a) {
                 }
                 const double sc = f[i] - (node >= 0 ? f[node] : 0.0);
                 if (m < a.min_chain_anchors || sc < a.min_chain_score) continue;
-                // spans over the members (original coordinates)
+                const int c = n_cand++;
+                a.c_score[a0 + c] = sc;
+                a.c_mem[a0 + c] = make_int2(moff, m);
+                a.c_strand[a0 + c] = (int8_t)(seg == 0 ? 1 : -1);
+                n_memtot += m;
+            }
+        }
+        __syncthreads();
+        // spans of this segment's chains over their members' original
+        // coordinates: one warp per chain, members 32 at a time
+        {
+            const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+            for (int c = c_first + wid; c < n_cand; c += nw) {
+                const int2 cm = a.c_mem[a0 + c];
                 int rs = 0x7fffffff, re = -0x7fffffff - 1, fs = 0x7fffffff, fe = -0x7fffffff - 1;
-                for (int x = 0; x < m; ++x) {
-                    const int o = a.perm[a0 + s0 + a.mem_tmp[a0 + moff + x]];
+                for (int x = lane; x < cm.y; x += 32) {
+                    const int o = a.perm[a0 + s0 + a.mem_tmp[a0 + cm.x + x]];
                     const int rp = a.read_pos[a0 + o], fp = a.ref_pos[a0 + o], ln = a.length[a0 + o];
                     rs = min(rs, rp);
                     re = max(re, rp + ln);
                     fs = min(fs, fp);
                     fe = max(fe, fp + ln);
                 }
-                const int c = n_cand++;
-                a.c_score[a0 + c] = sc;
-                a.c_span[a0 + c] = make_int4(rs, re, fs, fe);
-                a.c_mem[a0 + c] = make_int2(moff, m);
-                a.c_strand[a0 + c] = (int8_t)(seg == 0 ? 1 : -1);
-                n_memtot += m;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    rs = min(rs, __shfl_xor_sync(FULL_MASK, rs, o));
+                    re = max(re, __shfl_xor_sync(FULL_MASK, re, o));
+                    fs = min(fs, __shfl_xor_sync(FULL_MASK, fs, o));
+                    fe = max(fe, __shfl_xor_sync(FULL_MASK, fe, o));
+                }
+                if (lane == 0) a.c_span[a0 + c] = make_int4(rs, re, fs, fe);
             }
         }
         __syncthreads();
@@ -501,7 +527,11 @@ using namespace gmf;
 
 namespace {
 
-int sort_smem_elems() { return 8192; }  // 8192 * 12 B = 96 KB
+// Shared-memory sort buffers: 4096 keys (48 KB) for the per-read sort and
+// 2048 (24 KB) for the per-strand peel, so 4 and 9 CTAs fit an SM; larger
+// reads / strands sort in their own workspace range instead.
+int sort_smem_elems() { return 4096; }
+int peel_smem_elems() { return 2048; }
 
 size_t sort_smem_bytes(int elems) { return (size_t)elems * (sizeof(unsigned long long) + sizeof(int)); }
 
@@ -735,7 +765,7 @@ extern "C" int gmf_chain_batch(const gmf_anchor_batch* an, const gmf_chain_param
     k.c_mem = c_mem;
     k.c_strand = c_strand;
     k.claimed = c_strand + A;
-    k.smem_elems = sort_smem_elems();
+    k.smem_elems = peel_smem_elems();
     k.cap = (int64_t)A;
     k.n_chains = res->n_chains;
     k.score = res->score;
