@@ -83,6 +83,17 @@ class GmfSwTuning(Structure):
     ]
 
 
+class GmfMinimizerIndex(Structure):
+    _fields_ = [
+        ("k", c_int32),
+        ("w", c_int32),
+        ("n_keys", c_int64),
+        ("keys", c_void_p),
+        ("offsets", c_void_p),
+        ("positions", c_void_p),
+    ]
+
+
 class GmfChainParams(Structure):
     _fields_ = [
         ("max_lookback", c_int32),
@@ -140,6 +151,10 @@ _SIGNATURES = {
                                     c_void_p, c_size_t, c_void_p]),
     "gmf_gather_segments": (c_int, [c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_void_p,
                                     c_void_p, c_void_p]),
+    "gmf_seed_count": (c_int, [POINTER(GmfMinimizerIndex), c_int32, c_void_p, c_void_p, c_int32, c_void_p,
+                               c_void_p]),
+    "gmf_seed_fill": (c_int, [POINTER(GmfMinimizerIndex), c_int32, c_void_p, c_void_p, c_int32, c_void_p,
+                              c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "gmf_sw_get_tuning": (c_int, [POINTER(GmfSwTuning)]),
     "gmf_sw_set_tuning": (c_int, [POINTER(GmfSwTuning)]),
     "gmf_chain_dp": (c_int, [c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32,

@@ -156,6 +156,42 @@ int gmf_gather_segments(const int8_t* src, int64_t src_len, int32_t n, const int
                         const int32_t* len, const int8_t* rc, int8_t* dst, const int64_t* dst_off,
                         gmf_stream_t stream);
 
+/* ======================================================================== */
+/* Minimizer seeding                                                        */
+/* ======================================================================== */
+
+/* A (w, k) minimizer index of a reference, resident on the device: sorted
+ * unique packed k-mers (int64, 2 bits per base, A=0 .. T=3), CSR offsets and
+ * the ascending reference positions of each key -- the table
+ * alignment/seeding.py L202-254 (KmerTable.build) makes for MinimizerIndex
+ * L524-538, max_occ already applied. */
+typedef struct {
+    int32_t k;              /* 1..31 */
+    int32_t w;              /* 1..256 */
+    int64_t n_keys;
+    const int64_t* keys;
+    const int64_t* offsets; /* n_keys + 1 */
+    const int32_t* positions;
+} gmf_minimizer_index;
+
+/* Pass 1 of seeding a batch of reads (codes CSR, read_off[n_reads + 1]):
+ * counts[2r] = anchors of read r, counts[2r + 1] = anchors of its reverse
+ * complement (0 unless both_strands).  Replaces MinimizerIndex.query
+ * (seeding.py L540-545) applied per orientation by SeedingEngine.seed_read
+ * (L1056-1101) before diagonal merging. */
+int gmf_seed_count(const gmf_minimizer_index* index, int32_t n_reads, const int8_t* codes,
+                   const int64_t* read_off, int32_t both_strands, int64_t* counts, gmf_stream_t stream);
+
+/* Pass 2: the anchors, at anchor_off[2r] (forward) and anchor_off[2r + 1]
+ * (reverse complement, read_pos in the reverse-complemented read) with
+ * anchor_off the exclusive prefix sum of the counts (2 * n_reads + 1
+ * entries); within an orientation in the reference's order (read position,
+ * then reference position).  length = k, strand = +1 / -1. */
+int gmf_seed_fill(const gmf_minimizer_index* index, int32_t n_reads, const int8_t* codes,
+                  const int64_t* read_off, int32_t both_strands, const int64_t* anchor_off,
+                  int32_t* read_pos, int32_t* ref_pos, int32_t* length, int8_t* strand,
+                  gmf_stream_t stream);
+
 /* Scheduling knobs of the batched form (per device, process-wide).  They
  * decide which kernel shape aligns which pair and how the kernels overlap;
  * results never depend on them.  graphmambaformer_b200.autotune times

@@ -23,6 +23,10 @@ Fixtures:
   anchors of simulated HiFi reads.
 * ``extend_golden.npz`` -- ``ExtensionEngine.extend_chains`` on single-chain
   calls (window, band widening, soft clips).
+* ``seed_golden.npz``   -- ``MinimizerIndex`` (build + ``query``) on seeded
+  references with N runs and a repeated block, reads of many lengths (shorter
+  than k, with N bases, mutated copies) in both orientations, ``max_occ`` 0
+  and 5.
 * ``hybrid_golden.pkl`` -- ``AffineChainer.chain`` with a ``ChainingContext``
   (graph-distance oracle, backbone bias, neural seed scores with each AGNES
   trust decision, learned transitions).
@@ -451,6 +455,48 @@ def make_hybrid(rng):
     print(f"hybrid_golden.pkl: {len(reads)} reads, {sum(len(c) for c in out)} chains")
 
 
+def make_seed(rng):
+    from graphmambaformer.alignment.seeding import MinimizerIndex, reverse_complement_codes
+
+    cases = {}
+    refs, reads_all, params, out = [], [], [], {"read_pos": [], "ref_pos": [], "length": []}
+    for case, (ref_len, k, w, max_occ) in enumerate(((200_000, 15, 10, 0), (120_000, 11, 5, 5),
+                                                      (150_000, 19, 12, 0))):
+        ref = synth.random_reference(ref_len, rng)
+        ref[5000:5040] = 5  # an N run
+        blk = ref[20_000:20_400].copy()
+        for s0 in (40_000, 60_000, 80_000, 100_000, 110_000, 115_000):
+            ref[s0: s0 + 400] = blk  # a repeated block (caught by max_occ)
+        idx = MinimizerIndex(ref, k=k, window=w, max_occ=max_occ)
+        reads = [ref[1000:1010].copy(), ref[300:300 + k].copy()]
+        for L in (150, 1000, 5000, 20_000):
+            st = int(rng.integers(0, ref_len - L))
+            reads.append(synth.apply_errors(ref[st: st + L], synth.ONT, rng))
+        r = ref[20_000:20_600].copy()
+        r[100:103] = 5
+        reads.append(r)
+        for read in reads:
+            for strand, codes in ((1, read), (-1, reverse_complement_codes(read))):
+                a, b, c = idx.query(codes)
+                out["read_pos"].append(np.asarray(a, np.int64))
+                out["ref_pos"].append(np.asarray(b, np.int64))
+                out["length"].append(np.asarray(c, np.int64))
+                params.append((case, len(reads_all), strand))
+            reads_all.append(read)
+        refs.append((ref, k, w, max_occ))
+    cnt = np.array([len(x) for x in out["read_pos"]], np.int64)
+    aoff = np.zeros(len(cnt) + 1, np.int64)
+    np.cumsum(cnt, out=aoff[1:])
+    rq, roff = ragged(reads_all, np.int8)
+    fr, foff = ragged([x[0] for x in refs], np.int8)
+    np.savez_compressed(
+        os.path.join(HERE, "seed_golden.npz"),
+        ref=fr, ref_off=foff, ref_kw=np.array([[k, w, mo] for _, k, w, mo in refs], np.int64),
+        reads=rq, read_off=roff, query=np.array(params, np.int64), anchor_off=aoff,
+        read_pos=np.concatenate(out["read_pos"]), ref_pos=np.concatenate(out["ref_pos"]),
+        length=np.concatenate(out["length"]))
+
+
 if __name__ == "__main__":
     which = sys.argv[1:] or ["sw", "chain", "extend", "hybrid"]
     if "sw" in which:
@@ -461,3 +507,5 @@ if __name__ == "__main__":
         make_extend(np.random.default_rng(303))
     if "hybrid" in which:
         make_hybrid(np.random.default_rng(404))
+    if "seed" in which:
+        make_seed(np.random.default_rng(505))
