@@ -1,11 +1,13 @@
 """Serving loop: chaining + extension for a stream of read requests.
 
-A request carries 1..64 reads (base codes) and their raw minimizer anchors
-(seeding happens on the client).  The server keeps the reference codes and
-the chaining penalty table resident on the device and, per batch of reads,
-runs the two stages of the reference's classical path
-(alignment/chaining.py L620-745 then alignment/extension.py L469-641):
+A request carries 1..64 reads (base codes) and, when the server holds no
+minimizer index, their raw minimizer anchors (client-side seeding).  The
+server keeps the reference codes, the chaining penalty table and optionally
+the minimizer index resident on the device and, per batch of reads, runs the
+classical path (alignment/seeding.py L1056-1101 MinimizerIndex seeding, then
+alignment/chaining.py L620-745 and alignment/extension.py L469-641):
 
+  0. with an index: ``gmf_seed_count`` / ``gmf_seed_fill`` on the device;
   1. ``gmf_chain_batch``: strand split + sort, DP, chain peeling, select;
   2. the window and band of every kept chain (extension.py L489-509, on the
      host from the chain records), then ``gmf_gather_segments`` builds the
@@ -58,8 +60,9 @@ class BatchAligner:
     buffers, reused between batches)."""
 
     def __init__(self, ref_d: torch.Tensor, device, chain_cfg: ChainingConfig, ext_cfg: ExtensionConfig,
-                 stream: Optional[torch.cuda.Stream] = None):
+                 stream: Optional[torch.cuda.Stream] = None, index=None):
         self.device = require_cuda(device)
+        self.index = index  # a resident DeviceMinimizerIndex: seed on the device when no anchors are given
         self.ref_d = ref_d
         self.ref_len = int(ref_d.numel())
         self.ccfg, self.ecfg = chain_cfg, ext_cfg
@@ -73,16 +76,16 @@ class BatchAligner:
     def _call(self, name, *args):
         _native.check(name, getattr(_native.lib(), name)(*args))
 
-    def align(self, reads: Sequence[np.ndarray], anchors) -> list:
+    def align(self, reads: Sequence[np.ndarray], anchors=None) -> list:
         """Per read, the list of its chains' ExtensionResults (in select
         order), exactly as AffineChainer.chain + ExtensionEngine.extend_chains
-        give them."""
-        a = AnchorCSR.of(anchors)
+        give them.  Without ``anchors`` the reads are seeded on the device
+        against the resident minimizer index."""
         R = len(reads)
-        if R != len(a):
-            raise ValueError("one anchor set per read is required")
         if R == 0:
             return []
+        if anchors is None and self.index is None:
+            raise ValueError("anchors are required unless the aligner holds a minimizer index")
         s, up, db = self.stream, self.buf.upload, self.buf.device_buf
         sp = int(s.cuda_stream)
         bind(self.device, sp)
@@ -91,15 +94,26 @@ class BatchAligner:
         np.cumsum(rl, out=roff[1:])
         codes = np.concatenate(reads).astype(np.int8) if roff[-1] else np.zeros(1, np.int8)
         reads_d = up("reads", codes, s)
-        A = int(a.read_off[-1])
+        pad = lambda x, dt: x if len(x) else np.zeros(1, dt)  # noqa: E731
+        if anchors is None:  # device seeding: both orientations, forward anchors first
+            sd = self.index.seed_device(reads_d, up("roff", roff, s), R, True, stream=s)
+            ro, rp, fp, ln, st = sd["read_off"], sd["read_pos"], sd["ref_pos"], sd["length"], sd["strand"]
+            A = int(sd["n_anchors"])
+            with torch.cuda.stream(s):  # host copies for the window spans, after the fill on this stream
+                a = AnchorCSR(ro.cpu().numpy(), rp[:A].cpu().numpy(), fp[:A].cpu().numpy(), ln[:A].cpu().numpy(),
+                              st[:A].cpu().numpy())
+        else:
+            a = AnchorCSR.of(anchors)
+            if R != len(a):
+                raise ValueError("one anchor set per read is required")
+            A = int(a.read_off[-1])
+            ro = up("ro", a.read_off, s)
+            rp = up("rp", pad(a.read_pos, np.int32), s)
+            fp = up("fp", pad(a.ref_pos, np.int32), s)
+            ln = up("ln", pad(a.length, np.int32), s)
+            st = up("st", pad(a.strand, np.int8), s)
         if np.diff(a.read_off).max(initial=0) > _native.MAX_READ_ANCHORS:
             raise ValueError(f"a read has more than {_native.MAX_READ_ANCHORS} anchors")
-        pad = lambda x, dt: x if len(x) else np.zeros(1, dt)  # noqa: E731
-        ro = up("ro", a.read_off, s)
-        rp = up("rp", pad(a.read_pos, np.int32), s)
-        fp = up("fp", pad(a.ref_pos, np.int32), s)
-        ln = up("ln", pad(a.length, np.int32), s)
-        st = up("st", pad(a.strand, np.int8), s)
         mc = self.cp.max_chains
         o = dict(n=db("n", R, torch.int32), score=db("score", R * mc, torch.float64),
                  strand=db("strand", R * mc, torch.int32), span=db("span", 4 * R * mc, torch.int32),
@@ -230,7 +244,7 @@ class AlignServer:
 
     def __init__(self, ref_codes: np.ndarray, device=None, chain_cfg: Optional[ChainingConfig] = None,
                  ext_cfg: Optional[ExtensionConfig] = None, budget_bytes: int = 8 << 30,
-                 max_batch_reads: int = 512, workers: int = 2):
+                 max_batch_reads: int = 512, workers: int = 2, index=None):
         self.device = require_cuda(device)
         self.ccfg = chain_cfg or ChainingConfig()
         self.ecfg = ext_cfg or ExtensionConfig()
@@ -238,7 +252,9 @@ class AlignServer:
         self.max_batch_reads = int(max_batch_reads)
         torch.cuda.set_device(self.device)
         self.ref_d = torch.from_numpy(np.ascontiguousarray(ref_codes, np.int8)).to(self.device)  # resident
-        self.workers = [BatchAligner(self.ref_d, self.device, self.ccfg, self.ecfg) for _ in range(workers)]
+        self.index = index  # with a resident minimizer index, requests carry reads only
+        self.workers = [BatchAligner(self.ref_d, self.device, self.ccfg, self.ecfg, index=index)
+                        for _ in range(workers)]
         self.free: "queue.Queue[BatchAligner]" = queue.Queue()
         for w in self.workers:
             self.free.put(w)
@@ -253,10 +269,20 @@ class AlignServer:
         self._threads: list = []
 
     # -- client side -------------------------------------------------------------
-    def submit(self, reads: Sequence[np.ndarray], anchors) -> Future:
-        a = AnchorCSR.of(anchors)
-        nb = estimate_bytes(np.array([len(x) for x in reads], np.int64), int(a.read_off[-1]), self.ecfg,
-                            self.ccfg.max_chains)
+    def submit(self, reads: Sequence[np.ndarray], anchors=None) -> Future:
+        """Queue a request; ``anchors`` (per read, both orientations) are
+        required unless the server holds a minimizer index, in which case the
+        reads are seeded on the device and client anchors are not used."""
+        rl = np.array([len(x) for x in reads], np.int64)
+        if self.index is not None:
+            a = None
+            n_anchors = int(rl.sum() * 2 * 2 // (self.index.w + 1)) + 1  # minimizer density bound
+        else:
+            if anchors is None:
+                raise ValueError("anchors are required: the server has no minimizer index")
+            a = AnchorCSR.of(anchors)
+            n_anchors = int(a.read_off[-1])
+        nb = estimate_bytes(rl, n_anchors, self.ecfg, self.ccfg.max_chains)
         if nb > self.budget:
             raise ValueError("request larger than the working-memory budget")
         with self.lock:
@@ -317,8 +343,10 @@ class AlignServer:
     def _run(self, w: BatchAligner, batch: list, nbytes: int) -> None:
         try:
             reads = [r for req in batch for r in req.reads]
-            anchors = AnchorCSR.from_sets(
-                [_ReadAnchors(req.anchors, i) for req in batch for i in range(len(req.reads))])
+            anchors = None
+            if self.index is None:
+                anchors = AnchorCSR.from_sets(
+                    [_ReadAnchors(req.anchors, i) for req in batch for i in range(len(req.reads))])
             res = w.align(reads, anchors)
             pos = 0
             now = time.perf_counter()
@@ -364,6 +392,11 @@ class _ReadAnchors:
 
 
 def serve_stream(server: AlignServer, pool, requests: list, time_scale: float = 1.0) -> dict:
+    """Replay a request stream against a started server (see below)."""
+    return _serve_stream(server, pool, requests, time_scale)
+
+
+def _serve_stream(server: AlignServer, pool, requests: list, time_scale: float = 1.0) -> dict:
     """Replay a request stream (list of (arrival seconds, read indices)
     into ``pool``) against a started server, then wait for every result.
     Returns latency / throughput figures."""
@@ -374,7 +407,7 @@ def serve_stream(server: AlignServer, pool, requests: list, time_scale: float = 
         if wait > 0:
             time.sleep(wait)
         reads, anchors = pool.take(idx)
-        futs.append(server.submit(reads, anchors))
+        futs.append(server.submit(reads, None if server.index is not None else anchors))
     for f in futs:
         f.result(timeout=600)
     wall = time.perf_counter() - t0

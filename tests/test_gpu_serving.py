@@ -75,3 +75,29 @@ def test_serving_same_alone_and_in_the_mix(pool):
             assert len(ra) == len(rb) and all(_ext_equal(x, y) for x, y in zip(ra, rb))
     assert st["requests"] >= 3 * len(reqs) and st["p99_ms"] >= st["p50_ms"] > 0
     assert srv.batches < st["requests"]  # requests were batched together
+
+
+def test_device_seeding_server_matches_client_anchors(pool):
+    """A server holding the minimizer index seeds requests of bare reads on
+    the device and returns exactly what the client-side anchors give."""
+    from graphmambaformer_b200 import synth
+    from graphmambaformer_b200.seeding import DeviceMinimizerIndex
+    from graphmambaformer_b200.serving import AlignServer
+
+    reqs = synth.poisson_requests(12, reads_per_s=4000, pool_size=len(pool), seed=18, max_reads=12)
+    idx = DeviceMinimizerIndex(pool.ref, k=15, w=10, max_occ=200, device="cuda:0")
+    a_srv = AlignServer(pool.ref, "cuda:0", workers=2, max_batch_reads=40).start()
+    b_srv = AlignServer(pool.ref, "cuda:0", workers=2, max_batch_reads=40, index=idx).start()
+    try:
+        fa = [a_srv.submit(*pool.take(ix)) for _, ix in reqs]
+        fb = [b_srv.submit(pool.take(ix)[0]) for _, ix in reqs]  # reads only
+        ra = [f.result(timeout=300) for f in fa]
+        rb = [f.result(timeout=300) for f in fb]
+    finally:
+        a_srv.stop()
+        b_srv.stop()
+    assert sum(len(x) for r in ra for x in r) > 0
+    for x, y in zip(ra, rb):
+        assert len(x) == len(y)
+        for cx, cy in zip(x, y):
+            assert len(cx) == len(cy) and all(_ext_equal(p, q) for p, q in zip(cx, cy))
