@@ -60,7 +60,7 @@ def parse():
     p.add_argument("--no-autotune", action="store_true")
     p.add_argument("--long-reads", type=int, default=200,
                    help="reads of the long-read stress leg (2,000 = the full configuration; 0 skips it)")
-    p.add_argument("--serve-load", type=float, default=20_000.0, help="offered load of the serving leg, reads/s")
+    p.add_argument("--serve-loads", default="10000,20000", help="offered loads of the serving leg, reads/s")
     p.add_argument("--serve-requests", type=int, default=600)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile-case", action="store_true",
@@ -545,18 +545,22 @@ def serve_leg(args, device, seed: int) -> dict:
     pool = synth.mixed_read_pool(n_reads=2000, seed=seed, ref_len=10_000_000)
     index = DeviceMinimizerIndex(pool.ref, k=15, w=10, max_occ=200, device=device)
     srv = AlignServer(pool.ref, device, budget_bytes=8 << 30, workers=2, max_batch_reads=512, index=index).start()
+    loads = [float(x) for x in str(args.serve_loads).split(",") if x]
+    points = []
     try:
-        warm = synth.poisson_requests(40, args.serve_load, len(pool), seed=seed + 1)
+        warm = synth.poisson_requests(40, loads[0], len(pool), seed=seed + 1)
         serve_stream(srv, pool, warm)
-        srv.completed.clear()
-        srv.batches = 0
-        reqs = synth.poisson_requests(args.serve_requests, args.serve_load, len(pool), seed=seed + 2)
-        st = serve_stream(srv, pool, reqs)
+        for i, load in enumerate(loads):
+            srv.completed.clear()
+            srv.batches = 0
+            reqs = synth.poisson_requests(args.serve_requests, load, len(pool), seed=seed + 2 + i)
+            st = serve_stream(srv, pool, reqs)
+            points.append({"offered_reads_per_s": load, "achieved_reads_per_s": st["reads_per_s"],
+                           "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+                           "requests": st["requests"], "reads": st["reads"], "batches": st["batches"]})
     finally:
         srv.stop()
-    return {"offered_reads_per_s": args.serve_load, "achieved_reads_per_s": st["reads_per_s"],
-            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
-            "requests": st["requests"], "reads": st["reads"], "batches": st["batches"],
+    return {**points[-1], "loads": points,
             "config": {"reference": "10 Mb uniform and its (k=15, w=10) minimizer index, resident on the device",
                        "requests": "1-64 bare reads, Poisson arrivals; seeding, chaining and extension on the GPU",
                        "reads": "pool of 2,000 mixed-profile reads (150 bp - 20 kb)",

@@ -117,3 +117,29 @@ def test_stages_refuse_to_run_without_a_gpu():
     a = AnchorSet.from_lists([0, 20], [0, 20], [15, 15], [1, 1])
     with pytest.raises(RuntimeError, match="CUDA"):
         AffineChainer().chain(a)
+
+
+def test_entry_points_reject_malformed_arguments_before_any_cuda_call():
+    """Argument checks run on the host first, so these return the documented
+    status without a GPU."""
+    from graphmambaformer_b200 import _native
+    from graphmambaformer_b200.autotune import SwTuning
+
+    lib = _native.lib()
+    bad_idx = _native.GmfMinimizerIndex(0, 10, 0, None, None, None)  # k = 0
+    assert lib.gmf_seed_count(ctypes.byref(bad_idx), 1, None, None, 1, None, None) == _native.GMF_ERR_INVALID_ARGUMENT
+    big_w = _native.GmfMinimizerIndex(15, 300, 0, None, None, None)
+    assert lib.gmf_seed_fill(ctypes.byref(big_w), 1, None, None, 1, None, None, None, None, None, None) \
+        == _native.GMF_ERR_INVALID_ARGUMENT
+    assert lib.gmf_gather_segments(None, 0, -1, None, None, None, None, None, None) == _native.GMF_ERR_INVALID_ARGUMENT
+    assert lib.gmf_gather_segments(None, 10, 3, None, None, None, None, None, None) == _native.GMF_ERR_INVALID_ARGUMENT
+    assert lib.gmf_sw_set_tuning(ctypes.byref(SwTuning(130, 125).to_c())) == _native.GMF_ERR_INVALID_ARGUMENT
+    assert lib.gmf_sw_set_tuning(None) == _native.GMF_ERR_INVALID_ARGUMENT
+    batch = _native.GmfAnchorBatch(1, None, None, None, None, None)
+    cp = _native.GmfChainParams(64, 5000, 1, 8, 20.0, 0.5, 0.6)
+    res = _native.GmfChainResults(None, None, None, None, None, None, None)
+    assert lib.gmf_chain_batch_noalloc(ctypes.byref(batch), ctypes.byref(cp), None, 0, 10 ** 9, ctypes.byref(res),
+                                       None) == _native.GMF_ERR_LIMIT
+    assert lib.gmf_banded_sw(None, None, None, None, 0, None) == _native.GMF_ERR_INVALID_ARGUMENT
+    assert lib.gmf_chain_dp(-1, None, None, None, None, None, 64, 5000, None, 0, None, None, None) \
+        == _native.GMF_ERR_INVALID_ARGUMENT
