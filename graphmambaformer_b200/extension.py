@@ -401,8 +401,10 @@ class ExtensionEngine:
                 continue
             reverse = reverse_complement(forward)
             read_len, ref_len = len(forward), len(ref_codes)
-            for chain in chains:
-                start, end, hb = self._window(chain, anchors, read_len, ref_len)
+            windows = [self._window(chain, anchors, read_len, ref_len) for chain in chains]
+            # one band for every chain of the read: the widest (extension.py L534)
+            hb = max(w[2] for w in windows)
+            for chain, (start, end, _) in zip(chains, windows):
                 codes = forward if chain.strand > 0 else reverse
                 qs.append(codes)
                 ts.append(ref_codes[start:end])

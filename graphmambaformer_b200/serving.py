@@ -164,7 +164,10 @@ class BatchAligner:
         wend = np.minimum(self.ref_len, diag + rlen + cfg.flank)
         wend = np.where(wend - wstart > cfg.max_window, wstart + cfg.max_window, wend)
         wlen = np.maximum(wend - wstart, 0)
-        hb = np.minimum(cfg.half_band + spread, cfg.max_half_band).astype(np.int32)
+        hb_chain = np.minimum(cfg.half_band + spread, cfg.max_half_band)
+        hb_read = np.zeros(R, np.int64)
+        np.maximum.at(hb_read, cr, hb_chain)  # every chain of a read takes its widest band
+        hb = hb_read[cr].astype(np.int32)
         boff = (diag - wstart).astype(np.int32)
         qoff = np.zeros(C + 1, np.int64)
         np.cumsum(rlen, out=qoff[1:])

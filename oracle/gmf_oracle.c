@@ -22,6 +22,12 @@
  *   oracle_chain_backtrack chaining.py L530-576 (_backtrack: stable argsort
  *                         of -f, claimed mask, partial-chain score)
  *   oracle_chain_select   chaining.py L579-617 (select + _read_overlap)
+ *   oracle_wfa_align      extension.py L308-463 (WavefrontAligner.align +
+ *                         _traceback: unit-cost global wavefronts from
+ *                         diagonal 0, each candidate clipped on its own in
+ *                         the forward pass, completion checked before the
+ *                         max_distance test, traceback picks the first
+ *                         largest of X, I, D without clipping)
  *   oracle_chain_read     chaining.py L620-642 (chain: strand +1 then -1,
  *                         for_strand / sorted_by_ref from alignment/types.py
  *                         L144-152, weight = length, no bonus)
@@ -653,4 +659,106 @@ void oracle_chain_batch(int64_t n_reads, const int64_t* read_off, const int64_t*
     for (int k = 0; k < n_threads; ++k) pthread_create(&th[k], NULL, chain_worker, &job);
     for (int k = 0; k < n_threads; ++k) pthread_join(th[k], NULL);
     free(th);
+}
+
+
+/* ------------------------------------------------------------------------ */
+/* Wavefront alignment (unit edit costs, global)                            */
+/* ------------------------------------------------------------------------ */
+static int64_t wfa_extend(int64_t i, int64_t k, const int16_t* q, int64_t n, const int16_t* t, int64_t m) {
+    if (i < 0) return i;
+    int64_t j = i - k;
+    while (i < n && j >= 0 && j < m && q[i] == t[j] && q[i] >= 0 && q[i] != N_CODE) {
+        ++i;
+        ++j;
+    }
+    return i;
+}
+
+/* Edit distance and CIGAR words (run << 4 | op, op 0 '=', 1 'X', 2 'I',
+ * 3 'D'); returns the distance, -1 when it exceeds max_distance, -2 when
+ * out of memory.  *n_words receives the number of CIGAR words (cigar must
+ * hold n + m + 2). */
+int64_t oracle_wfa_align(const int16_t* q, int64_t n, const int16_t* t, int64_t m, int64_t max_distance,
+                         uint32_t* cigar, int64_t* n_words) {
+    *n_words = 0;
+    if (n == 0 || m == 0) {
+        if (n > 0) cigar[(*n_words)++] = ((uint32_t)n << 4) | 2u;
+        if (m > 0) cigar[(*n_words)++] = ((uint32_t)m << 4) | 3u;
+        return n > m ? n : m;
+    }
+    const int64_t final_k = n - m;
+    /* history: wavefront s covers diagonals [-s, s], stored at s*s */
+    int64_t cap = 1024;
+    int64_t* H = (int64_t*)malloc(sizeof(int64_t) * cap);
+    if (!H) return -2;
+    H[0] = wfa_extend(0, 0, q, n, t, m);
+    int64_t score = 0;
+    for (;;) {
+        /* completion of wavefront `score` */
+        if (-score <= final_k && final_k <= score && H[score * score + (final_k + score)] >= n) break;
+        if (score >= max_distance) {
+            free(H);
+            return -1;
+        }
+        ++score;
+        const int64_t need = (score + 1) * (score + 1);
+        if (need > cap) {
+            while (cap < need) cap *= 2;
+            int64_t* H2 = (int64_t*)realloc(H, sizeof(int64_t) * cap);
+            if (!H2) {
+                free(H);
+                return -2;
+            }
+            H = H2;
+        }
+        const int64_t* prev = H + (score - 1) * (score - 1);
+        const int64_t ps = score - 1;
+        int64_t* cur = H + score * score;
+        for (int64_t k = -score; k <= score; ++k) {
+            int64_t cand[3];
+            const int64_t pk[3] = {k, k - 1, k + 1};
+            for (int c = 0; c < 3; ++c) {
+                const int64_t idx = pk[c] + ps;
+                int64_t v = (idx >= 0 && idx <= 2 * ps) ? prev[idx] : -1;
+                if (c < 2) v = v >= 0 ? v + 1 : -1; /* substitution, insertion consume a query base */
+                const int64_t col = v - k;
+                if (v < 0 || v > n || col < 0 || col > m) v = -1;
+                cand[c] = v;
+            }
+            int64_t best = cand[0] > cand[1] ? cand[0] : cand[1];
+            best = best > cand[2] ? best : cand[2];
+            cur[k + score] = wfa_extend(best, k, q, n, t, m);
+        }
+    }
+    /* traceback */
+    unsigned char* ops = (unsigned char*)malloc((size_t)(n + m + 2));
+    if (!ops) {
+        free(H);
+        return -2;
+    }
+    int64_t n_ops = 0, k = final_k;
+    for (int64_t s = score; s >= 1; --s) {
+        const int64_t reach = H[s * s + (k + s)];
+        const int64_t* prev = H + (s - 1) * (s - 1);
+        const int64_t ps = s - 1;
+        const int64_t pk[3] = {k, k - 1, k + 1};
+        int64_t val[3];
+        for (int c = 0; c < 3; ++c) {
+            const int64_t idx = pk[c] + ps;
+            const int64_t v = (idx >= 0 && idx <= 2 * ps && prev[idx] >= 0) ? prev[idx] : -1;
+            val[c] = c < 2 ? (v >= 0 ? v + 1 : -1) : v;
+        }
+        int best = 0; /* first largest: X, then I, then D */
+        for (int c = 1; c < 3; ++c)
+            if (val[c] > val[best]) best = c;
+        for (int64_t x = 0; x < reach - val[best]; ++x) ops[n_ops++] = 0; /* '=' */
+        ops[n_ops++] = (unsigned char)(best == 0 ? 1 : (best == 1 ? 2 : 3));
+        k = pk[best];
+    }
+    for (int64_t x = 0; x < H[k + 0]; ++x) ops[n_ops++] = 0; /* score-0 match run (k == 0) */
+    *n_words = rle_reverse(ops, n_ops, cigar);
+    free(ops);
+    free(H);
+    return score;
 }

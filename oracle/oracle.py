@@ -54,6 +54,7 @@ def lib() -> ctypes.CDLL:
         if not os.path.exists(path):
             build_oracle.build()
         _lib = ctypes.CDLL(path)
+        _lib.oracle_wfa_align.restype = ctypes.c_int64
     return _lib
 
 
@@ -263,3 +264,20 @@ def chain_batch(read_off, read_pos, ref_pos, length, strand, lut, max_lookback=6
         _p(out.strand), _p(out.span), _p(out.primary), _p(out.n_members), _p(out.members),
         _p(out.n_chains))
     return out
+
+
+def wfa_align(query: np.ndarray, target: np.ndarray, max_distance: int) -> tuple[int, list]:
+    """WavefrontAligner.align (extension.py L353-463): (edit distance, CIGAR
+    runs); distance -1 when it exceeds ``max_distance`` (where the reference
+    raises RuntimeError)."""
+    q = np.ascontiguousarray(query, np.int16)
+    t = np.ascontiguousarray(target, np.int16)
+    words = np.zeros(len(q) + len(t) + 2, np.uint32)
+    nw = ctypes.c_int64(0)
+    d = lib().oracle_wfa_align(_p(q), ctypes.c_int64(len(q)), _p(t), ctypes.c_int64(len(t)),
+                               ctypes.c_int64(int(max_distance)), _p(words), ctypes.byref(nw))
+    if d == -2:
+        raise MemoryError("oracle_wfa_align: out of memory")
+    if d < 0:
+        return -1, []
+    return int(d), [(OPS[w & 15], int(w >> 4)) for w in words[: nw.value]]

@@ -27,6 +27,14 @@ Fixtures:
   references with N runs and a repeated block, reads of many lengths (shorter
   than k, with N bases, mutated copies) in both orientations, ``max_occ`` 0
   and 5.
+* ``wfa_golden.npz``    -- ``WavefrontAligner.align`` (distance + CIGAR, or
+  the over-budget signal) on the reference's own cases
+  (tests/test_alignment_stages.py L1063-1111, tests/test_accel.py L336-345)
+  and seeded pairs (empty sides, N bases, every error profile, lengths up to
+  3000, several distance budgets), plus ``ExtensionEngine.extend_chains``
+  calls with several chains per read, in ``banded_sw`` mode (one band shared
+  by the read's chains) and in ``wfa`` mode (window from the chain's
+  diagonal and net indel, banded-SW fallback beyond ``wfa_max_distance``).
 * ``hybrid_golden.pkl`` -- ``AffineChainer.chain`` with a ``ChainingContext``
   (graph-distance oracle, backbone bias, neural seed scores with each AGNES
   trust decision, learned transitions).
@@ -497,6 +505,118 @@ def make_seed(rng):
         length=np.concatenate(out["length"]))
 
 
+# --------------------------------------------------------------------------- #
+# WavefrontAligner + multi-chain extend_chains (both algorithms)
+# --------------------------------------------------------------------------- #
+def make_wfa(rng):
+    from graphmambaformer.alignment.extension import WavefrontAligner
+
+    # ---- aligner cases: (query, target, max_distance) ----
+    cases = [("ACGTACGTACGT", "ACGTACGTACGT", 4096), ("ACGT", "TGCA", 4096), ("AN", "AN", 4096),
+             ("ACGTAC", "ACGTTAC", 4), ("", "", 4096), ("", "ACG", 4096), ("ACGTA", "", 4096),
+             ("NNNN", "NNNN", 4096), ("A", "C", 0), ("A", "A", 0), ("ACGT", "ACGA", 1)]
+    cases = [(encode_bases(a), encode_bases(b), d) for a, b, d in cases]
+    for _ in range(3):  # unrelated sequences past a small budget (L1094-1103)
+        cases.append((synth.random_reference(60, rng).astype(np.int8),
+                       synth.random_reference(60, rng).astype(np.int8), 2))
+    profiles = (synth.ILLUMINA, synth.HIFI, synth.ONT)
+    for c in range(150):
+        L = int(rng.choice([int(rng.integers(1, 40)), int(rng.integers(40, 400)), int(rng.integers(400, 3000))]))
+        a = synth.random_reference(L, rng).astype(np.int8)
+        b = synth.apply_errors(a, profiles[c % 3], rng).astype(np.int8)
+        if c % 7 == 0 and L > 10:
+            a[rng.integers(0, L, size=max(1, L // 50))] = 5
+        if c % 5 == 0:
+            b = np.concatenate([b, synth.random_reference(int(rng.integers(1, 30)), rng).astype(np.int8)])
+        if c % 9 == 0:
+            a, b = b, a
+        md = int(rng.choice([4096, 4096, 50, 8]))
+        cases.append((a, b, md))
+    qs, ts, mds, dist, cig = [], [], [], [], []
+    for a, b, md in cases:
+        wfa = WavefrontAligner(ExtensionConfig(algorithm="wfa", wfa_max_distance=md))
+        try:
+            d, cigar = wfa.align(np.asarray(a, np.int8), np.asarray(b, np.int8))
+        except RuntimeError:
+            d, cigar = -1, []
+        qs.append(a)
+        ts.append(b)
+        mds.append(md)
+        dist.append(d)
+        cig.append(cigar_words(cigar))
+    q_flat, q_off = ragged(qs, np.int8)
+    t_flat, t_off = ragged(ts, np.int8)
+    c_flat, c_off = ragged(cig, np.uint32)
+
+    # ---- extend_chains with several chains per read ----
+    ref = synth.random_reference(400_000, rng)
+    ref_str = synth.decode_bases(ref)
+    reads, anc, chain_rows, call_rows, results = [], [], [], [], []
+    for call in range(48):
+        algo = call % 2  # 0 banded_sw, 1 wfa
+        prof = profiles[(call // 2) % 3]
+        L = int(rng.integers(100, 2500 if prof is synth.ILLUMINA else 4000))
+        s0 = int(rng.integers(300, len(ref) - L - 300))
+        strand = 1 if (call // 6) % 2 == 0 else -1
+        tmpl = ref[s0: s0 + L]
+        read = synth.apply_errors(tmpl if strand > 0 else synth.reverse_complement(tmpl), prof, rng)
+        oriented = read if strand > 0 else synth.reverse_complement(read)
+        n = len(oriented)
+        rp_l, fp_l, ln_l, st_l, rows = [], [], [], [], []
+        n_chains = int(rng.integers(1, 4))
+        for c in range(n_chains):
+            if c == 0:  # the true chain: anchors along the true diagonal
+                k = int(rng.integers(2, 6))
+                rp = np.sort(rng.choice(np.arange(0, max(n - 20, 1)), size=min(k, max(n - 20, 1)), replace=False))
+                fp = s0 + rp + rng.integers(-4, 5, size=len(rp))
+                cs = strand
+            else:  # a secondary chain elsewhere, possibly the other strand, wider spread
+                k = int(rng.integers(2, 5))
+                rp = np.sort(rng.choice(np.arange(0, max(n - 20, 1)), size=min(k, max(n - 20, 1)), replace=False))
+                base = int(rng.integers(500, len(ref) - n - 500))
+                fp = base + rp + rng.integers(-40, 41, size=len(rp))
+                cs = strand if rng.random() < 0.5 else -strand
+            lo = len(np.concatenate(rp_l)) if rp_l else 0
+            rp_l.append(rp.astype(np.int64))
+            fp_l.append(fp.astype(np.int64))
+            ln_l.append(np.full(len(rp), 15, np.int64))
+            st_l.append(np.full(len(rp), cs, np.int8))
+            rows.append((call, lo, lo + len(rp), cs))
+        rp, fp, ln, st = (np.concatenate(x) for x in (rp_l, fp_l, ln_l, st_l))
+        anchors = AnchorSet.from_lists(rp, fp, ln, st)
+        chains = [Chain(anchor_idx=np.arange(lo, hi), score=30.0, strand=cs,
+                        read_start=int(rp[lo:hi].min()), read_end=int((rp[lo:hi] + ln[lo:hi]).max()),
+                        ref_start=int(fp[lo:hi].min()), ref_end=int((fp[lo:hi] + ln[lo:hi]).max()))
+                  for (_, lo, hi, cs) in rows]
+        md = int(rng.choice([4096, 4096, 30]))
+        cfg = ExtensionConfig(algorithm="wfa" if algo else "banded_sw", wfa_max_distance=md)
+        eng = ExtensionEngine(cfg, device="cpu", backend="torch")
+        out = eng.extend_chains(synth.decode_bases(read), chains, anchors, ref_str)
+        reads.append(read)
+        anc.append(np.stack([rp, fp, ln, st.astype(np.int64)], 1))
+        chain_rows.extend(rows)
+        call_rows.append((algo, md))
+        results.extend(out)
+    r_flat, r_off = ragged(reads, np.int8)
+    a_flat = np.concatenate(anc)
+    a_off = np.zeros(len(anc) + 1, np.int64)
+    np.cumsum([len(x) for x in anc], out=a_off[1:])
+    x_flat, x_off = ragged([cigar_words(x.cigar) for x in results], np.uint32)
+    np.savez_compressed(
+        os.path.join(HERE, "wfa_golden.npz"),
+        q=q_flat, q_off=q_off, t=t_flat, t_off=t_off, max_distance=np.array(mds, np.int64),
+        distance=np.array(dist, np.int64), cigar=c_flat, cigar_off=c_off,
+        ref=ref, reads=r_flat, read_off=r_off, anchors=a_flat, anchor_off=a_off,
+        chains=np.array(chain_rows, np.int64), calls=np.array(call_rows, np.int64),
+        x_score=np.array([x.score for x in results], np.float64),
+        x_span=np.array([[x.read_start, x.read_end, x.ref_start, x.ref_end] for x in results], np.int64),
+        x_counts=np.array([[x.n_match, x.n_mismatch, x.n_insertion, x.n_deletion] for x in results], np.int64),
+        x_cigar=x_flat, x_cigar_off=x_off,
+    )
+    print(f"wfa_golden.npz: {len(cases)} aligner cases ({sum(d < 0 for d in dist)} over budget), "
+          f"{len(call_rows)} extend calls, {len(results)} chains")
+
+
 if __name__ == "__main__":
     which = sys.argv[1:] or ["sw", "chain", "extend", "hybrid"]
     if "sw" in which:
@@ -509,3 +629,5 @@ if __name__ == "__main__":
         make_hybrid(np.random.default_rng(404))
     if "seed" in which:
         make_seed(np.random.default_rng(505))
+    if "wfa" in which:
+        make_wfa(np.random.default_rng(606))

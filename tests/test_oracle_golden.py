@@ -119,3 +119,52 @@ def test_chain_known_answer():
     f, p = oracle.chain_dp([10, 20, 30], [10, 20, 31], [10.5, 9.25, 8.75], lut)
     assert p.tolist() == [-1, 0, 1]
     assert f[0] == 10.5 and f[1] == 10.5 + 9.25
+
+
+def _levenshtein(a, b):
+    prev = list(range(len(b) + 1))
+    for i, ca in enumerate(a, 1):
+        cur = [i]
+        for j, cb in enumerate(b, 1):
+            same = ca == cb and 0 <= ca != 5
+            cur.append(min(prev[j] + 1, cur[j - 1] + 1, prev[j - 1] + (0 if same else 1)))
+        prev = cur
+    return prev[-1]
+
+
+def test_wfa_oracle_matches_reference_golden(golden_dir):
+    """oracle_wfa_align against WavefrontAligner.align (distance, CIGAR and
+    the over-budget signal) on every golden case."""
+    g = _load(golden_dir, "wfa_golden.npz")
+    for i in range(len(g["distance"])):
+        q = g["q"][g["q_off"][i]: g["q_off"][i + 1]]
+        t = g["t"][g["t_off"][i]: g["t_off"][i + 1]]
+        d, cigar = oracle.wfa_align(q, t, int(g["max_distance"][i]))
+        assert d == g["distance"][i], i
+        assert cigar == _words_to_cigar(g["cigar"][g["cigar_off"][i]: g["cigar_off"][i + 1]]), i
+
+
+def test_wfa_oracle_is_levenshtein():
+    """The reference's own property (tests/test_alignment_stages.py L1063-1091):
+    distance == Levenshtein, and the CIGAR consumes both sequences with
+    exactly `distance` edits."""
+    rng = np.random.default_rng(7)
+    for _ in range(60):
+        a = rng.integers(1, 6, size=int(rng.integers(0, 40))).astype(np.int16)
+        b = a.copy().tolist()
+        for _ in range(int(rng.integers(0, 6))):
+            pos = int(rng.integers(0, len(b) + 1))
+            act = int(rng.integers(0, 3))
+            if act == 0 and pos < len(b):
+                b[pos] = int(rng.integers(1, 6))
+            elif act == 1 and pos < len(b):
+                b.pop(pos)
+            else:
+                b.insert(pos, int(rng.integers(1, 6)))
+        b = np.array(b, np.int16)
+        d, cigar = oracle.wfa_align(a, b, 4096)
+        assert d == _levenshtein(a.tolist(), b.tolist())
+        assert sum(n for op, n in cigar if op in "=XI") == len(a)
+        assert sum(n for op, n in cigar if op in "=XD") == len(b)
+        if len(a) and len(b):
+            assert sum(n for op, n in cigar if op in "XID") == d
