@@ -25,6 +25,7 @@ GMF_ERR_NOT_READY = 7
 GMF_SWF_WORKSPACE = 1
 GMF_SWF_CAPACITY = 2
 GMF_SWF_TIMEOUT = 4
+GMF_SWF_INTERNAL = 8
 
 MAX_HALF_BAND = 4096
 MAX_READ_ANCHORS = 16384
@@ -139,6 +140,34 @@ class GmfChainResults(Structure):
     ]
 
 
+class GmfWfaPairs(Structure):
+    _fields_ = [
+        ("n_pairs", c_int32),
+        ("query", c_void_p),
+        ("query_off", c_void_p),
+        ("target", c_void_p),
+        ("target_off", c_void_p),
+        ("order", c_void_p),
+        ("query_total", c_int64),
+        ("target_total", c_int64),
+        ("max_len", c_int32),
+    ]
+
+
+class GmfWfaResults(Structure):
+    _fields_ = [
+        ("op_counts", c_void_p),
+        ("cigar", c_void_p),
+        ("cigar_capacity", c_int64),
+        ("cigar_start", c_void_p),
+        ("cigar_len", c_void_p),
+        ("cigar_used", c_void_p),
+        ("error_flags", c_void_p),
+    ]
+
+
+MAX_WFA_DISTANCE = 1 << 16
+
 # name -> (restype, argtypes)
 _SIGNATURES = {
     "gmf_status_string": (c_char_p, [c_int]),
@@ -167,6 +196,11 @@ _SIGNATURES = {
                                 POINTER(GmfChainResults), c_void_p, c_size_t, c_void_p]),
     "gmf_chain_batch_noalloc": (c_int, [POINTER(GmfAnchorBatch), POINTER(GmfChainParams), c_void_p,
                                         c_int32, c_int64, POINTER(GmfChainResults), c_void_p]),
+    "gmf_wfa_workspace_bytes": (c_size_t, [c_int32, c_int32, c_int32, c_int64]),
+    "gmf_wfa_history_entries": (c_int64, [c_int32, c_void_p, c_void_p, c_void_p]),
+    "gmf_wfa_distance": (c_int, [POINTER(GmfWfaPairs), c_int32, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "gmf_wfa_align": (c_int, [POINTER(GmfWfaPairs), c_void_p, c_int32, POINTER(GmfWfaResults), c_void_p,
+                              c_size_t, c_void_p]),
 }
 
 _lib = None

@@ -430,15 +430,66 @@ class ExtensionEngine:
 
     def extend_batch(self, reads: Sequence[str], chains_per_read, anchor_sets, ref_seq: str) -> list:
         """``extend_chains`` for many reads in one device launch."""
-        if self.cfg.algorithm != "banded_sw":
-            raise NotImplementedError(f"algorithm {self.cfg.algorithm!r} is not built on the B200 path")
         ref_codes = self._ref.get(ref_seq)
         items = [(encode_bases(r), c, a, ref_codes) for r, c, a in zip(reads, chains_per_read, anchor_sets)]
+        if self.cfg.algorithm == "wfa":
+            return self._extend_wfa(items)
+        return self._extend_sw(items)
+
+    def _extend_sw(self, items) -> list:
         ps, meta = self._pairs(items)
-        results: list = [[] for _ in reads]
+        results: list = [[] for _ in items]
         if len(ps) == 0:
             return results
         res = align_pairs(ps, params_from_config(self.cfg), traceback=True, device=self.device)
         for (r, _, _), ext in zip(meta, self._finish(res, meta)):
             results[r].append(ext)
+        return results
+
+    def _extend_wfa(self, items) -> list:
+        """WFA mode (extension.py L643-730): each chain is aligned end to end
+        against the reference stretch its read-zero diagonal and net indel
+        imply; a chain beyond ``wfa_max_distance`` falls back to banded SW of
+        that chain alone.  The score is recomputed from the CIGAR with the
+        affine parameters."""
+        from .wfa import align_wfa_pairs
+
+        cfg = self.cfg
+        qs, ts, meta = [], [], []
+        for r, (forward, chains, anchors, ref_codes) in enumerate(items):
+            if not chains:
+                continue
+            reverse = reverse_complement(forward)
+            read_len, ref_len = len(forward), len(ref_codes)
+            for ci, chain in enumerate(chains):
+                codes = forward if chain.strand > 0 else reverse
+                start = int(np.clip(chain.ref_start - chain.read_start, 0, max(ref_len - 1, 0)))
+                net_indel = chain.ref_span - chain.read_span
+                end = min(ref_len, start + max(1, read_len + net_indel))
+                qs.append(codes)
+                ts.append(ref_codes[start:end])
+                meta.append((r, ci, start, read_len))
+        results: list = [[None] * len(it[1]) for it in items]
+        if not meta:
+            return [[] for _ in items]
+        res = align_wfa_pairs(qs, ts, cfg.wfa_max_distance, device=self.device)
+        fallback = []
+        for b, (r, ci, start, read_len) in enumerate(meta):
+            if res.distance[b] < 0:
+                forward, chains, anchors, ref_codes = items[r]
+                fallback.append(((r, ci), (forward, [chains[ci]], anchors, ref_codes)))
+                continue
+            cigar = res.cigar(b)
+            counts = {op: 0 for op in ("=", "X", "I", "D")}
+            for op, n in cigar:
+                counts[op] = counts.get(op, 0) + n
+            gap_cost = sum(cfg.gap_open + max(n - 1, 0) * cfg.gap_extend for op, n in cigar if op in ("I", "D"))
+            score = counts["="] * cfg.match_score - counts["X"] * cfg.mismatch_penalty - gap_cost
+            results[r][ci] = ExtensionResult(
+                score=float(score), cigar=cigar, read_start=0, read_end=read_len, ref_start=start,
+                ref_end=start + len(ts[b]), n_match=counts["="], n_mismatch=counts["X"],
+                n_insertion=counts["I"], n_deletion=counts["D"])
+        if fallback:  # banded SW, one chain per call as the reference re-enters extend_chains
+            for (r, ci), ext in zip((k for k, _ in fallback), self._extend_sw([it for _, it in fallback])):
+                results[r][ci] = ext[0]
         return results

@@ -26,6 +26,8 @@
  *   gmf_chain_sort    alignment/types.py L144-152 (for_strand, sorted_by_ref)
  *   gmf_chain_batch   alignment/chaining.py L620-745 (AffineChainer.chain /
  *                     chain_batch: sort, DP, _backtrack, select)
+ *   gmf_wfa_distance  accel/cuda_kernels.py L569-600 (wfa_distance)
+ *   gmf_wfa_align     alignment/extension.py L308-463 (WavefrontAligner)
  */
 #ifndef GMF_ALIGN_H
 #define GMF_ALIGN_H
@@ -122,6 +124,8 @@ typedef struct {
 #define GMF_SWF_CAPACITY 2u  /* cigar_capacity exceeded */
 #define GMF_SWF_TIMEOUT 4u   /* a bounded wait between the warps sharing a pair gave up (that
                                 pair's result is unreliable); not expected in normal operation */
+#define GMF_SWF_INTERNAL 8u  /* an internal consistency check failed (a distance that does not
+                                belong to the pair); the pair is reported without a CIGAR */
 
 /* Bytes of workspace gmf_banded_sw needs for a batch.  HOST arrays. */
 size_t gmf_banded_sw_workspace_bytes(int32_t n_pairs, const int32_t* query_len,
@@ -326,6 +330,71 @@ int gmf_chain_batch(const gmf_anchor_batch* anchors, const gmf_chain_params* par
 int gmf_chain_batch_noalloc(const gmf_anchor_batch* anchors, const gmf_chain_params* params,
                             const double* pen_lut, int32_t lut_len, int64_t n_anchors,
                             const gmf_chain_results* results, gmf_stream_t stream);
+
+/* ======================================================================== */
+/* Unit-cost global wavefront alignment (WFA)                               */
+/* ======================================================================== */
+
+#define GMF_MAX_WFA_DISTANCE (1 << 16) /* distance bound of a call */
+
+/* Pairs aligned end to end (codes and matching as in gmf_pairs). */
+typedef struct {
+    int32_t n_pairs;
+    const int8_t* query;       /* concatenated query codes */
+    const int64_t* query_off;  /* n_pairs+1 offsets into query */
+    const int8_t* target;      /* concatenated target codes */
+    const int64_t* target_off; /* n_pairs+1 offsets into target */
+    const int32_t* order;      /* optional processing order (a permutation); NULL = 0..n-1.
+                                  It changes scheduling only, never results. */
+    int64_t query_total;       /* HOST value: query_off[n_pairs] */
+    int64_t target_total;      /* HOST value: target_off[n_pairs] */
+    int32_t max_len;           /* HOST value >= every query and target length */
+} gmf_wfa_pairs;
+
+/* Per-pair outputs of gmf_wfa_align.  The CIGAR of pair p is
+ * cigar[cigar_start[p] .. + cigar_len[p]) as words (run << 4) | op, op 0 '=',
+ * 1 'X', 2 'I', 3 'D', packed densely in completion order; cigar_len[p] is -1
+ * when the pair has no alignment (distance -1), its history did not fit the
+ * workspace (GMF_SWF_WORKSPACE) or its words did not fit cigar_capacity
+ * (GMF_SWF_CAPACITY). */
+typedef struct {
+    int32_t* op_counts;          /* 4 per pair (= X I D) or NULL */
+    uint32_t* cigar;
+    int64_t cigar_capacity;      /* words available in cigar (n + m + 1 per pair always suffice) */
+    int64_t* cigar_start;        /* per pair */
+    int32_t* cigar_len;          /* per pair */
+    unsigned long long* cigar_used; /* one device word, written by the call */
+    int32_t* error_flags;        /* one device word: OR of GMF_SWF_* flags (written by the call) */
+} gmf_wfa_results;
+
+/* Bytes of workspace for a WFA call: gmf_wfa_distance needs
+ * history_entries = 0; gmf_wfa_align needs the total of (d+1)^2 over its pairs
+ * (gmf_wfa_history_entries), or less, in which case the pairs that do not fit
+ * are reported and can be retried.  max_distance: the call's bound
+ * (gmf_wfa_align: >= every distance). */
+size_t gmf_wfa_workspace_bytes(int32_t n_pairs, int32_t max_len, int32_t max_distance,
+                               int64_t history_entries);
+
+/* Sum over pairs of (distance+1)^2 (pairs with distance -1 or an empty side
+ * count 0).  HOST arrays; -1 on a bad argument. */
+int64_t gmf_wfa_history_entries(int32_t n_pairs, const int32_t* query_len, const int32_t* target_len,
+                                const int32_t* distance);
+
+/* Edit distance of every pair, or -1 when it exceeds max_distance (where the
+ * reference raises).  An empty side answers max(n, m) whatever the bound.
+ * Replaces accel/cuda_kernels.py L569-600 (wfa_distance) and the distance of
+ * alignment/extension.py L353-408 (WavefrontAligner.align). */
+int gmf_wfa_distance(const gmf_wfa_pairs* pairs, int32_t max_distance, int32_t* distance,
+                     void* workspace, size_t workspace_bytes, gmf_stream_t stream);
+
+/* CIGAR of every pair from the distances of a prior gmf_wfa_distance (device
+ * array) on the same pairs: the wavefronts are recomputed to that distance
+ * with their history kept, then walked back (ties: X, then I, then D).
+ * max_distance: HOST value >= every distance[p].  Replaces
+ * alignment/extension.py L410-463 (WavefrontAligner._traceback). */
+int gmf_wfa_align(const gmf_wfa_pairs* pairs, const int32_t* distance, int32_t max_distance,
+                  const gmf_wfa_results* results, void* workspace, size_t workspace_bytes,
+                  gmf_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -73,6 +73,8 @@ int main(void) {
   P(gmf_chain_params); O(gmf_chain_params, min_chain_score);
   P(gmf_anchor_batch); O(gmf_anchor_batch, strand);
   P(gmf_sorted_anchors); P(gmf_chain_results); O(gmf_chain_results, members);
+  P(gmf_wfa_pairs); O(gmf_wfa_pairs, query_total); O(gmf_wfa_pairs, max_len);
+  P(gmf_wfa_results); O(gmf_wfa_results, cigar_capacity); O(gmf_wfa_results, error_flags);
   return 0;
 }
 """
@@ -101,6 +103,12 @@ def test_ctypes_structs_match_c_layout(tmp_path):
         "gmf_sorted_anchors": ctypes.sizeof(n.GmfSortedAnchors),
         "gmf_chain_results": ctypes.sizeof(n.GmfChainResults),
         "gmf_chain_results.members": n.GmfChainResults.members.offset,
+        "gmf_wfa_pairs": ctypes.sizeof(n.GmfWfaPairs),
+        "gmf_wfa_pairs.query_total": n.GmfWfaPairs.query_total.offset,
+        "gmf_wfa_pairs.max_len": n.GmfWfaPairs.max_len.offset,
+        "gmf_wfa_results": ctypes.sizeof(n.GmfWfaResults),
+        "gmf_wfa_results.cigar_capacity": n.GmfWfaResults.cigar_capacity.offset,
+        "gmf_wfa_results.error_flags": n.GmfWfaResults.error_flags.offset,
     }
     for k, v in want.items():
         assert int(got[k]) == v, (k, got[k], v)
@@ -143,3 +151,19 @@ def test_entry_points_reject_malformed_arguments_before_any_cuda_call():
     assert lib.gmf_banded_sw(None, None, None, None, 0, None) == _native.GMF_ERR_INVALID_ARGUMENT
     assert lib.gmf_chain_dp(-1, None, None, None, None, None, 64, 5000, None, 0, None, None, None) \
         == _native.GMF_ERR_INVALID_ARGUMENT
+    # WFA: bounds and malformed pairs, all refused on the host
+    bad_pairs = _native.GmfWfaPairs(2, None, None, None, None, None, 10, 10, 5)
+    assert lib.gmf_wfa_distance(ctypes.byref(bad_pairs), 8, None, None, 0, None) == _native.GMF_ERR_INVALID_ARGUMENT
+    empty = _native.GmfWfaPairs(0, None, None, None, None, None, 0, 0, 0)
+    assert lib.gmf_wfa_distance(ctypes.byref(empty), _native.MAX_WFA_DISTANCE + 1, None, None, 0, None) \
+        == _native.GMF_ERR_LIMIT
+    assert lib.gmf_wfa_align(ctypes.byref(empty), None, -1, None, None, 0, None) == _native.GMF_ERR_LIMIT
+    assert lib.gmf_wfa_distance(None, 8, None, None, 0, None) == _native.GMF_ERR_INVALID_ARGUMENT
+    import numpy as np
+
+    ql = np.array([10, 0, 5], np.int32)
+    tl = np.array([12, 7, 5], np.int32)
+    dist = np.array([3, 7, -1], np.int32)
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    assert lib.gmf_wfa_history_entries(3, p(ql), p(tl), p(dist)) == 16
+    assert lib.gmf_wfa_workspace_bytes(3, 12, 8, 16) >= lib.gmf_wfa_workspace_bytes(3, 12, 8, 0) + 64
