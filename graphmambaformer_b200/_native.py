@@ -44,6 +44,8 @@ class GmfPairs(Structure):
         ("band_offset", c_void_p),
         ("order", c_void_p),
         ("max_half_band", c_int32),
+        ("xdrop_group_off", c_void_p),
+        ("n_xdrop_groups", c_int32),
     ]
 
 

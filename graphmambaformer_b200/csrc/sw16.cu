@@ -392,6 +392,7 @@ __device__ void sw16_group(const SwArgs& a, int p, const Grp<L>& grp, uint32_t* 
 
     int bh, bi, bd;
     if (XD) {
+        if (active && k == 0) record_rowmax(a, p, rowmax);
         xdrop_best<L>(grp, rowmax, qlen, a.x_drop, active, bh, bi, bd);
     } else {
         lane_best16<L>(lb, pos0, pos1, K.Z, k, P, bh, bi, bd);
@@ -637,6 +638,7 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* pro
     }
     if (w != 0) return;
     if (XD) {
+        if (lane == 0) record_rowmax(a, p, rowmax);
         xdrop_best<L>(grp, rowmax, qlen, a.x_drop, true, bh, bi, bd);
     } else {
         bh = sbest[0][0];

@@ -162,6 +162,7 @@ __device__ void sw32_pair(const SwArgs& a, int p, const Grp<32>& grp, int2* ring
 
     int bh, bi, bd;
     if (XD) {
+        if (lane == 0) record_rowmax(a, p, rowmax);
         xdrop_best<32>(grp, rowmax, qlen, a.x_drop, true, bh, bi, bd);
     } else {
         bh = lb;

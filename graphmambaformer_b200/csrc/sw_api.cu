@@ -93,7 +93,9 @@ static size_t round_up(size_t x, size_t m) { return (x + m - 1) / m * m; }
 // Queue heads and counts, the class lists, and the per-pair traceback
 // location (base word, layout tag) the deferred walk reads.
 static size_t queue_bytes(int n_pairs) {
+    // heads/counts, class lists, walk records (base, tag), group x-drop records (row maxima, carry)
     return round_up(2 * N_CLASSES * sizeof(int32_t), 256) + round_up((size_t)N_CLASSES * n_pairs * 4, 256) +
+           round_up((size_t)n_pairs * 8, 256) + round_up((size_t)n_pairs * 4, 256) +
            round_up((size_t)n_pairs * 8, 256) + round_up((size_t)n_pairs * 4, 256);
 }
 
@@ -179,6 +181,7 @@ static int check_common(const gmf_pairs* pairs, const gmf_sw_params* params, con
     if (pairs->n_pairs > 0 && (!pairs->query || !pairs->query_off || !pairs->target ||
                                !pairs->target_off || !pairs->half_band || !pairs->band_offset))
         return GMF_ERR_INVALID_ARGUMENT;
+    if (pairs->xdrop_group_off && pairs->n_xdrop_groups < 0) return GMF_ERR_INVALID_ARGUMENT;
     return GMF_OK;
 }
 
@@ -244,6 +247,96 @@ static int warps_per_block(size_t per_warp, const DevInfo& di, int cap = 4) {
     return per_warp > (size_t)di.smem_optin ? 0 : wpb;
 }
 
+// Group x-drop (alignment/extension.py L139-193 on a batch of several pairs):
+// the row loop stops after the first row on which every member satisfies
+// (max row max so far) - row max > x_drop, a member's rows past its query
+// reading as 0; each member's best is then the first strictly larger row max
+// over the rows up to that one.  One warp per group of two or more members
+// (a pair alone already stopped on its own rows), rows in chunks of 32: a
+// prefix max over the lanes plus the member's carry gives the running max.
+__global__ void __launch_bounds__(128) sw_xdrop_group_kernel(SwArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int gw = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const int nw = (int)((gridDim.x * (unsigned)blockDim.x) >> 5);
+    for (int g = gw; g < a.n_xg; g += nw) {
+        const int lo = max(a.xg_off[g], 0), hi = min(a.xg_off[g + 1], a.n_pairs);
+        if (hi - lo <= 1) continue;
+        int max_rows = 0;
+        for (int p = lo; p < hi; ++p) max_rows = max(max_rows, (int)(a.q_off[p + 1] - a.q_off[p]));
+        for (int p = lo + lane; p < hi; p += 32) a.rm_seen[p] = 0;
+        __syncwarp();
+        // pass 1: the last row the batch considers
+        int stop = max_rows - 1;
+        for (int r0 = 0; r0 < max_rows; r0 += 32) {
+            const int r = r0 + lane;
+            unsigned all = __ballot_sync(FULL_MASK, r < max_rows);
+            for (int p = lo; p < hi; ++p) {
+                const unsigned long long rb_at = a.rm_base[p];
+                const int ql = (int)(a.q_off[p + 1] - a.q_off[p]);
+                const int2* rm = rb_at == ~0ull ? nullptr : reinterpret_cast<const int2*>(a.pool + rb_at);
+                const int rb = (rm && r < ql) ? rm[r].x : 0;
+                int pm = rb;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int u = __shfl_up_sync(FULL_MASK, pm, o);
+                    if (lane >= o) pm = imax(pm, u);
+                }
+                pm = imax(pm, a.rm_seen[p]);
+                all &= __ballot_sync(FULL_MASK, pm - rb > a.x_drop);
+                const int carry = __shfl_sync(FULL_MASK, pm, 31);
+                __syncwarp();
+                if (lane == 0) a.rm_seen[p] = carry;
+                __syncwarp();
+            }
+            if (all) {
+                stop = r0 + __ffs((int)all) - 1;
+                break;
+            }
+        }
+        // pass 2: each member's best over rows [0, min(stop, qlen-1)]
+        for (int p = lo; p < hi; ++p) {
+            const unsigned long long rb_at = a.rm_base[p];
+            if (rb_at == ~0ull) continue;  // no rows: the class kernel's empty result stands
+            const int2* rm = reinterpret_cast<const int2*>(a.pool + rb_at);
+            const int ql = (int)(a.q_off[p + 1] - a.q_off[p]);
+            const int last = imin(stop, ql - 1);
+            int bh = 0, bi = 0, bd = 0;
+            for (int r0 = 0; r0 <= last; r0 += 32) {
+                const int r = r0 + lane;
+                const int2 v = r <= last ? rm[r] : make_int2(-1, 0);
+                int cv = v.x, cl = lane;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const int ov = __shfl_xor_sync(FULL_MASK, cv, o);
+                    const int ol = __shfl_xor_sync(FULL_MASK, cl, o);
+                    if (ov > cv || (ov == cv && ol < cl)) {
+                        cv = ov;
+                        cl = ol;
+                    }
+                }
+                const int cd = __shfl_sync(FULL_MASK, v.y, cl);
+                if (cv > bh) {
+                    bh = cv;
+                    bi = r0 + cl + 1;
+                    bd = cd;
+                }
+            }
+            if (lane == 0) {
+                const int hb = a.hb[p], off = a.boff[p];
+                a.score[p] = bh;
+                a.q_end[p] = bh > 0 ? bi : 0;
+                a.t_end[p] = bh > 0 ? bi + off - hb + bd : 0;
+            }
+        }
+    }
+}
+
+static int launch_xdrop_groups(const SwArgs& a, int sms, cudaStream_t stream) {
+    const long long warps = std::min<long long>(a.n_xg, (long long)sms * 16);
+    sw_xdrop_group_kernel<<<(int)((warps + 3) / 4), 128, 0, stream>>>(a);
+    return cuda_status(cudaGetLastError());
+}
+
 }  // namespace gmf
 
 using namespace gmf;
@@ -288,6 +381,14 @@ static int sw_prepare(const gmf_pairs* pairs, const gmf_sw_params* params, const
     a.defer_walk = 0;
     if (pairs->n_pairs > 0)
         GMF_CUDA_TRY(cudaMemsetAsync(a.tb_tag, 0xFF, (size_t)pairs->n_pairs * 4, stream));
+    char* rm = tb + round_up((size_t)pairs->n_pairs * 8, 256) + round_up((size_t)pairs->n_pairs * 4, 256);
+    const bool groups = params->x_drop > 0 && pairs->xdrop_group_off && pairs->n_xdrop_groups > 0 &&
+                        pairs->n_pairs > 0;
+    a.xg_off = groups ? pairs->xdrop_group_off : nullptr;
+    a.n_xg = groups ? pairs->n_xdrop_groups : 0;
+    a.rm_base = groups ? (unsigned long long*)rm : nullptr;
+    a.rm_seen = groups ? (int32_t*)(rm + round_up((size_t)pairs->n_pairs * 8, 256)) : nullptr;
+    if (groups) GMF_CUDA_TRY(cudaMemsetAsync(a.rm_base, 0xFF, (size_t)pairs->n_pairs * 8, stream));
     a.pool = (uint32_t*)(w + 256 + qb);
     a.pool_cap = (workspace_bytes - 256 - qb) / 4;
     return GMF_OK;
@@ -380,6 +481,7 @@ extern "C" int gmf_banded_sw(const gmf_pairs* pairs, const gmf_sw_params* params
         GMF_CUDA_TRY(cudaEventRecord(ss->join[i], ss->s[i]));
         GMF_CUDA_TRY(cudaStreamWaitEvent(stream, ss->join[i], 0));
     }
+    if (a.n_xg > 0) GMF_TRY(launch_xdrop_groups(a, di.sms, stream));
     return tb ? launch_sw_walk(a, stream) : GMF_OK;
 }
 
@@ -397,8 +499,13 @@ extern "C" int gmf_banded_sw_plain(const gmf_pairs* pairs, const gmf_sw_params* 
     const int wpb = warps_per_block((size_t)sw32_smem_per_warp(a.ring), di);
     if (wpb == 0) return GMF_ERR_LIMIT;
     const int grid = (pairs->n_pairs + wpb - 1) / wpb;
-    return launch_sw32(a, res->cigar != nullptr, params->x_drop > 0, e_mode_of(params), false, grid,
-                       wpb, stream);
+    const bool tb = res->cigar != nullptr;
+    if (a.n_xg == 0) return launch_sw32(a, tb, params->x_drop > 0, e_mode_of(params), false, grid, wpb, stream);
+    // x-drop groups: the group pass settles each member's best before the walk
+    a.defer_walk = tb ? 1 : 0;
+    GMF_TRY(launch_sw32(a, tb, true, e_mode_of(params), false, grid, wpb, stream));
+    GMF_TRY(launch_xdrop_groups(a, di.sms, stream));
+    return tb ? launch_sw_walk(a, stream) : GMF_OK;
 }
 
 extern "C" int gmf_sw_get_tuning(gmf_sw_tuning* t) {

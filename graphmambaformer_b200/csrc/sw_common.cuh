@@ -59,6 +59,10 @@ struct SwArgs {
     int32_t cmin[3];                 // classifier: fewest strips of the 2-, 4-, 8-warp classes (0: off)
     unsigned long long* tb_base;     // per pair: first traceback word (pool offset)
     int32_t* tb_tag;                 // per pair: traceback layout (0 int32, L for 16x2), -1 none
+    const int32_t* xg_off;           // x-drop groups (n_xg+1 offsets), or null
+    int32_t n_xg;
+    unsigned long long* rm_base;     // per pair: row maxima (pool offset), ~0 none; null without groups
+    int32_t* rm_seen;                // per pair: running row max carried between row chunks
 };
 
 // Traceback-bit layout of the int32 form: one 32-bit word per lane per 8
@@ -79,6 +83,11 @@ struct Layout32 {
 __device__ __forceinline__ void record_walk(const SwArgs& a, int p, const uint32_t* bits, int tag) {
     a.tb_base[p] = (unsigned long long)(bits - a.pool);
     a.tb_tag[p] = tag;
+}
+
+// Where the group x-drop pass finds the row maxima of pair p.
+__device__ __forceinline__ void record_rowmax(const SwArgs& a, int p, const int2* rowmax) {
+    if (a.rm_base) a.rm_base[p] = (unsigned long long)(reinterpret_cast<const uint32_t*>(rowmax) - a.pool);
 }
 
 // Pipeline period of the 16x2 form: steps per strip of 2L rows, a multiple of

@@ -12,11 +12,13 @@ Drop-in for the reference's extension stage:
   (``_window`` + ``extend_chains``), the object the pipeline holds as
   ``pipeline.extender``.
 
-Semantics are the reference's, applied per pair: each pair uses its own band
-and its own x-drop, so its result does not depend on its batch-mates (the
-reference applies one band to all chains of a read and stops a batch only
-when every row dropped; its result for a pair equals this one when the pair
-is aligned alone, which is what the parity tests check).  Scores are integers
+Semantics are the reference's.  At the primitive level each pair carries its
+own band (the reference's scalar band is the special case), and x-drop stops
+a batch's row loop only after every member dropped: ``banded_affine_sw_batch``
+treats its whole batch as one x-drop group, ``ExtensionEngine`` one read's
+chains (which also share the widest band of the read, extension.py L534), and
+``align_pairs`` takes the groups a caller gives (``PairSet.xdrop_group_off``;
+none = each pair alone).  Scores are integers
 (float32 in the reference, exact below 2**24) and scoring parameters must be
 integral.  Every computation runs in the gmf CUDA library; without a GPU the
 calls raise.
@@ -90,6 +92,8 @@ class DevicePairs:
     h_tlen: np.ndarray
     h_hb: np.ndarray
     device: torch.device
+    xdrop_group_off: Optional[torch.Tensor] = None  # n_groups+1 offsets, or None
+    n_groups: int = 0
 
     @property
     def h2d_bytes(self) -> int:
@@ -117,6 +121,11 @@ def upload_pairs(pairs: PairSet, device=None, order: Optional[np.ndarray] = None
         order = longest_first(qlen, hb)
     q = pairs.query if len(pairs.query) else np.zeros(1, np.int8)
     t = pairs.target if len(pairs.target) else np.zeros(1, np.int8)
+    goff = None
+    if pairs.xdrop_group_off is not None:
+        goff = np.asarray(pairs.xdrop_group_off, np.int32)
+        if goff.ndim != 1 or len(goff) < 1 or goff[0] != 0 or goff[-1] != len(hb) or np.any(np.diff(goff) < 0):
+            raise ValueError("xdrop_group_off must rise from 0 to the number of pairs")
     return DevicePairs(
         n=len(hb),
         query=to_device(q.astype(np.int8, copy=False), dev),
@@ -127,7 +136,9 @@ def upload_pairs(pairs: PairSet, device=None, order: Optional[np.ndarray] = None
         band_offset=to_device(np.asarray(pairs.band_offset, dtype=np.int32), dev),
         order=None if order is None else to_device(np.asarray(order, dtype=np.int32), dev),
         max_half_band=int(hb.max()) if len(hb) else 0,
-        h_qlen=qlen, h_tlen=tlen, h_hb=hb, device=dev)
+        h_qlen=qlen, h_tlen=tlen, h_hb=hb, device=dev,
+        xdrop_group_off=None if goff is None else to_device(goff, dev),
+        n_groups=0 if goff is None else len(goff) - 1)
 
 
 @dataclass
@@ -189,7 +200,8 @@ def launch_banded_sw(dp: DevicePairs, params: _native.GmfSwParams, traceback: bo
     sp = stream_handle(stream, dp.device)
     bind(dp.device, sp)
     pairs = _native.GmfPairs(dp.n, ptr(dp.query), ptr(dp.query_off), ptr(dp.target), ptr(dp.target_off),
-                             ptr(dp.half_band), ptr(dp.band_offset), ptr(dp.order), dp.max_half_band)
+                             ptr(dp.half_band), ptr(dp.band_offset), ptr(dp.order), dp.max_half_band,
+                             ptr(dp.xdrop_group_off), dp.n_groups)
     res = _native.GmfSwResults(
         ptr(out.score), ptr(out.query_end), ptr(out.target_end), ptr(out.query_start),
         ptr(out.target_start), ptr(out.op_counts), ptr(out.cigar),
@@ -321,6 +333,7 @@ def banded_affine_sw_batch(query: torch.Tensor, target: torch.Tensor, query_len,
     dev = require_cuda(query.device if query.is_cuda else None)
     hb = cfg.half_band if half_band is None else half_band
     ps = _padded_to_pairs(query, target, query_len, target_len, hb, band_offset)
+    ps.xdrop_group_off = np.array([0, len(ps)], np.int32)  # one row loop for the whole batch
     dp = upload_pairs(ps, dev)
     res = fetch(launch_banded_sw(dp, params_from_config(cfg), bool(return_matrices)), dp.n)
     return BandedSWResult(
@@ -396,9 +409,11 @@ class ExtensionEngine:
         """items: (forward codes, chains, anchors, ref codes) per read ->
         PairSet + per-pair (read index, window start, read_len)."""
         qs, ts, hbs, offs, meta = [], [], [], [], []
+        groups = [0]
         for r, (forward, chains, anchors, ref_codes) in enumerate(items):
             if not chains:
                 continue
+            groups.append(groups[-1] + len(chains))
             reverse = reverse_complement(forward)
             read_len, ref_len = len(forward), len(ref_codes)
             windows = [self._window(chain, anchors, read_len, ref_len) for chain in chains]
@@ -411,7 +426,10 @@ class ExtensionEngine:
                 hbs.append(hb)
                 offs.append((chain.ref_start - chain.read_start) - start)
                 meta.append((r, start, read_len))
-        return PairSet.from_lists(qs, ts, np.array(hbs, np.int32), np.array(offs, np.int32)), meta
+        ps = PairSet.from_lists(qs, ts, np.array(hbs, np.int32), np.array(offs, np.int32))
+        # the chains of a read share the x-drop stop, as in the reference's batch (extension.py L190-193)
+        ps.xdrop_group_off = np.array(groups, np.int32)
+        return ps, meta
 
     def _finish(self, res: SWResult, meta) -> list:
         out = []

@@ -51,6 +51,8 @@ class GraphedAligner:
         self.h_hb, self.d_hb = pair(P, torch.int32)
         self.h_off, self.d_off = pair(P, torch.int32)
         self.h_ord, self.d_ord = pair(P, torch.int32)
+        # x-drop groups padded to P (trailing groups empty), so the captured count never changes
+        self.h_go, self.d_go = pair(P + 1, torch.int32)
         i32 = dict(dtype=torch.int32, device=dev)
         self.o = {k: torch.zeros(P, **i32) for k in ("score", "qe", "te", "qs", "ts", "clen")}
         self.o["counts"] = torch.zeros(4 * P, **i32)
@@ -88,6 +90,15 @@ class GraphedAligner:
         order = np.arange(P, dtype=np.int32)
         if n:
             order[:n] = longest_first(qlen, hb)
+        go = np.full(P + 1, n, np.int32)
+        g = pairs.xdrop_group_off
+        if g is None:
+            go[: n + 1] = np.arange(n + 1, dtype=np.int32)
+        else:
+            g = np.asarray(g, np.int32)
+            if len(g) - 1 > P or g[0] != 0 or g[-1] != n or np.any(np.diff(g) < 0):
+                raise ValueError("xdrop_group_off must rise from 0 to the number of pairs")
+            go[: len(g)] = g
         nq, nt = int(pairs.query_off[-1]), int(pairs.target_off[-1])
         if nq:
             self.h_q[:nq].numpy()[...] = pairs.query.astype(np.int8, copy=False)
@@ -98,6 +109,7 @@ class GraphedAligner:
         self.h_hb.numpy()[...] = hbp
         self.h_off.numpy()[...] = offp
         self.h_ord.numpy()[...] = order
+        self.h_go.numpy()[...] = go
         # workspace this batch needs (the padding pairs need none)
         need = int(_native.lib().gmf_banded_sw_workspace_bytes(
             P, np.ascontiguousarray(qo[1:] - qo[:-1], np.int32).ctypes.data_as(ctypes.c_void_p),
@@ -108,12 +120,13 @@ class GraphedAligner:
     # -- the captured sequence -------------------------------------------------
     def _sequence(self) -> None:
         for h, d in ((self.h_q, self.d_q), (self.h_t, self.d_t), (self.h_qo, self.d_qo), (self.h_to, self.d_to),
-                     (self.h_hb, self.d_hb), (self.h_off, self.d_off), (self.h_ord, self.d_ord)):
+                     (self.h_hb, self.d_hb), (self.h_off, self.d_off), (self.h_ord, self.d_ord),
+                     (self.h_go, self.d_go)):
             d.copy_(h, non_blocking=True)
         o, tb = self.o, self.traceback
         pairs_c = _native.GmfPairs(self.cap_pairs, self.d_q.data_ptr(), self.d_qo.data_ptr(), self.d_t.data_ptr(),
                                    self.d_to.data_ptr(), self.d_hb.data_ptr(), self.d_off.data_ptr(),
-                                   self.d_ord.data_ptr(), self.max_hb)
+                                   self.d_ord.data_ptr(), self.max_hb, self.d_go.data_ptr(), self.cap_pairs)
         res_c = _native.GmfSwResults(
             o["score"].data_ptr(), o["qe"].data_ptr(), o["te"].data_ptr(),
             o["qs"].data_ptr() if tb else None, o["ts"].data_ptr() if tb else None,

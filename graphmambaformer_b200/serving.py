@@ -201,8 +201,12 @@ class BatchAligner:
             C, rlen.astype(np.int32).ctypes.data_as(ctypes.c_void_p),
             wlen.astype(np.int32).ctypes.data_as(ctypes.c_void_p), hb.ctypes.data_as(ctypes.c_void_p), 1))
         sws = db("sws", need, torch.uint8)
+        # the chains of a read stop together under x-drop (pairs are in read order)
+        goff = np.zeros(R + 1, np.int32)
+        np.cumsum(n_ch, out=goff[1:])
+        go_d = up("go", goff, s)
         pairs_c = _native.GmfPairs(C, qd.data_ptr(), qo_d.data_ptr(), td.data_ptr(), to_d.data_ptr(), hb_d.data_ptr(),
-                                   bo_d.data_ptr(), ord_d.data_ptr(), int(hb.max()))
+                                   bo_d.data_ptr(), ord_d.data_ptr(), int(hb.max()), go_d.data_ptr(), R)
         sres = _native.GmfSwResults(out["score"].data_ptr(), out["qe"].data_ptr(), out["te"].data_ptr(),
                                     out["qs"].data_ptr(), out["ts"].data_ptr(), out["counts"].data_ptr(),
                                     cigar.data_ptr(), cap, out["cstart"].data_ptr(), out["clen"].data_ptr(),

@@ -113,9 +113,12 @@ class ExtensionSession:
             B, qlen.ctypes.data_as(ctypes.c_void_p), tlen.ctypes.data_as(ctypes.c_void_p),
             hb.ctypes.data_as(ctypes.c_void_p), 1 if self.traceback else 0))
         ws = db("ws", need, torch.uint8)
+        goff = pairs.xdrop_group_off
+        gd = up("goff", np.asarray(goff, np.int32), s) if goff is not None else None
         pairs_c = _native.GmfPairs(B, q.data_ptr(), qo.data_ptr(), t.data_ptr(), to.data_ptr(),
                                    hbd.data_ptr(), off.data_ptr(), od.data_ptr() if B else None,
-                                   int(hb.max()) if B else 0)
+                                   int(hb.max()) if B else 0, gd.data_ptr() if gd is not None else None,
+                                   len(goff) - 1 if goff is not None else 0)
         tb = self.traceback
         res_c = _native.GmfSwResults(
             out["score"].data_ptr(), out["qe"].data_ptr(), out["te"].data_ptr(),

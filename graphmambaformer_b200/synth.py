@@ -123,6 +123,9 @@ class PairSet:
     band_offset: np.ndarray  # int32 (B,)
     profile: Optional[np.ndarray] = None  # int8 per pair (0 illumina, 1 hifi, 2 ont)
     meta: dict = field(default_factory=dict)
+    # x-drop groups: pairs [off[g], off[g+1]) stop together (the reference's
+    # batch rule, e.g. the chains of one read); None = each pair alone
+    xdrop_group_off: Optional[np.ndarray] = None
 
     def __len__(self) -> int:
         return len(self.half_band)

@@ -97,6 +97,14 @@ typedef struct {
                                   0..n_pairs-1, e.g. longest first); NULL = 0..n-1.
                                   It changes scheduling only, never results. */
     int32_t max_half_band;     /* HOST value >= every half_band[p] (sizes shared memory) */
+    /* Optional x-drop groups (used only when x_drop > 0): pairs
+     * [xdrop_group_off[g], xdrop_group_off[g+1]) are aligned as one batch of
+     * the reference's row loop, which stops after the first row on which
+     * EVERY member has dropped (rows past a member's query read as 0), so a
+     * member keeps improving while another has not dropped.  Offsets are
+     * non-decreasing from 0 to n_pairs.  NULL = every pair is its own group. */
+    const int32_t* xdrop_group_off; /* n_xdrop_groups+1 offsets, device */
+    int32_t n_xdrop_groups;
 } gmf_pairs;
 
 /* Per-pair outputs.  Ends are 1-based (0 when score == 0), starts 0-based,

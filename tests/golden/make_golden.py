@@ -35,6 +35,10 @@ Fixtures:
   calls with several chains per read, in ``banded_sw`` mode (one band shared
   by the read's chains) and in ``wfa`` mode (window from the chain's
   diagonal and net indel, banded-SW fallback beyond ``wfa_max_distance``).
+* ``xdrop_golden.npz``  -- the batch x-drop rule: ``banded_affine_sw_batch``
+  batches whose members drop on different rows (small ``x_drop``), and
+  ``extend_chains`` on reads with unalignable blocks next to secondary
+  chains, where a chain keeps extending while another has not dropped.
 * ``hybrid_golden.pkl`` -- ``AffineChainer.chain`` with a ``ChainingContext``
   (graph-distance oracle, backbone bias, neural seed scores with each AGNES
   trust decision, learned transitions).
@@ -617,6 +621,120 @@ def make_wfa(rng):
           f"{len(call_rows)} extend calls, {len(results)} chains")
 
 
+# --------------------------------------------------------------------------- #
+# x-drop over a batch (all members must have dropped)
+# --------------------------------------------------------------------------- #
+def make_xdrop(rng):
+    # ---- banded_affine_sw_batch: batches of 2-5 pairs, x_drop 20..60 ----
+    bq, bt, bhb, boff, bgrp, bxd, out = [], [], [], [], [0], [], []
+    for batch in range(24):
+        B = int(rng.integers(2, 6))
+        xd = float(rng.choice([20.0, 35.0, 60.0]))
+        hb = int(rng.integers(4, 24))
+        qs, ts, offs = [], [], []
+        for _ in range(B):
+            L = int(rng.integers(60, 400))
+            t = synth.random_reference(L + 40, rng).astype(np.int8)
+            q = t[20: 20 + L].copy()
+            # a block of junk of random length somewhere: the pair drops there
+            if rng.random() < 0.8:
+                a0 = int(rng.integers(0, L))
+                jl = len(q[a0: a0 + int(rng.integers(10, 80))])
+                q[a0: a0 + jl] = synth.random_reference(jl, rng)
+            q = synth.apply_errors(q, synth.ILLUMINA, rng).astype(np.int8)
+            qs.append(q)
+            ts.append(t)
+            offs.append(20)
+        M = max(len(x) for x in qs)
+        N = max(len(x) for x in ts)
+        qt = torch.full((B, M), -1, dtype=torch.int16)
+        tt = torch.full((B, N), -1, dtype=torch.int16)
+        for b in range(B):
+            qt[b, : len(qs[b])] = torch.as_tensor(qs[b].astype(np.int16))
+            tt[b, : len(ts[b])] = torch.as_tensor(ts[b].astype(np.int16))
+        cfg = ExtensionConfig(x_drop=xd)
+        res = banded_affine_sw_batch(qt, tt, torch.tensor([len(x) for x in qs]), torch.tensor([len(x) for x in ts]),
+                                     cfg, half_band=hb, band_offset=torch.tensor(offs), return_matrices=True)
+        for b in range(B):
+            ext = traceback_banded(res, b, qs[b], ts[b], cfg)
+            out.append(dict(score=float(res.score[b]), qe=int(res.query_end[b]), te=int(res.target_end[b]),
+                            qs=int(ext.read_start), ts=int(ext.ref_start), cigar=cigar_words(ext.cigar)))
+        bq += qs
+        bt += ts
+        bhb += [hb] * B
+        boff += offs
+        bgrp.append(bgrp[-1] + B)
+        bxd.append(xd)
+
+    # ---- extend_chains: reads with unalignable blocks + secondary chains ----
+    ref = synth.random_reference(200_000, rng)
+    ref_str = synth.decode_bases(ref)
+    eng = ExtensionEngine(ExtensionConfig(), device="cpu", backend="torch")  # x_drop 600
+    reads, anc, chain_rows, results = [], [], [], []
+    for call in range(10):
+        A = int(rng.integers(300, 700))
+        J = int(rng.integers(900, 1600))
+        Bn = int(rng.integers(300, 900))
+        s0 = int(rng.integers(1000, len(ref) - 5000))
+        read = ref[s0: s0 + A + J + Bn].copy()
+        read[A: A + J] = synth.random_reference(J, rng)
+        read = synth.apply_errors(read, synth.HIFI, rng).astype(np.int8)
+        n = len(read)
+        rp = np.array([5, A // 2, A + J + 10, n - 40], np.int64)
+        fp = s0 + rp
+        rows = [(call, 0, 4, 1)]
+        n_sec = int(rng.integers(1, 3))
+        rp_l, fp_l = [rp], [fp]
+        for c in range(n_sec):
+            r2 = np.sort(rng.choice(np.arange(0, n - 20), size=2, replace=False)).astype(np.int64)
+            base = int(rng.integers(500, len(ref) - n - 500))
+            f2 = base + r2 + rng.integers(-20, 21, size=2)
+            lo = sum(len(x) for x in rp_l)
+            rp_l.append(r2)
+            fp_l.append(f2)
+            rows.append((call, lo, lo + 2, 1))
+        if call % 3 == 2:  # the read alone, one chain (the pair's own stop)
+            rows = rows[:1]
+            rp_l, fp_l = rp_l[:1], fp_l[:1]
+        rpa, fpa = np.concatenate(rp_l), np.concatenate(fp_l)
+        ln = np.full(len(rpa), 15, np.int64)
+        st = np.ones(len(rpa), np.int8)
+        anchors = AnchorSet.from_lists(rpa, fpa, ln, st)
+        chains = [Chain(anchor_idx=np.arange(lo, hi), score=30.0, strand=1,
+                        read_start=int(rpa[lo:hi].min()), read_end=int((rpa[lo:hi] + 15).max()),
+                        ref_start=int(fpa[lo:hi].min()), ref_end=int((fpa[lo:hi] + 15).max()))
+                  for (_, lo, hi, _) in rows]
+        res = eng.extend_chains(synth.decode_bases(read), chains, anchors, ref_str)
+        reads.append(read)
+        anc.append(np.stack([rpa, fpa, ln, st.astype(np.int64)], 1))
+        chain_rows.extend(rows)
+        results.extend(res)
+    q_flat, q_off = ragged(bq, np.int8)
+    t_flat, t_off = ragged(bt, np.int8)
+    c_flat, c_off = ragged([o["cigar"] for o in out], np.uint32)
+    r_flat, r_off = ragged(reads, np.int8)
+    a_flat = np.concatenate(anc)
+    a_off = np.zeros(len(anc) + 1, np.int64)
+    np.cumsum([len(x) for x in anc], out=a_off[1:])
+    x_flat, x_off = ragged([cigar_words(x.cigar) for x in results], np.uint32)
+    np.savez_compressed(
+        os.path.join(HERE, "xdrop_golden.npz"),
+        query=q_flat, query_off=q_off, target=t_flat, target_off=t_off, half_band=np.array(bhb, np.int32),
+        band_offset=np.array(boff, np.int32), batch_off=np.array(bgrp, np.int64), x_drop=np.array(bxd),
+        score=np.array([o["score"] for o in out]), qe=np.array([o["qe"] for o in out]),
+        te=np.array([o["te"] for o in out]), qs=np.array([o["qs"] for o in out]),
+        ts=np.array([o["ts"] for o in out]), cigar=c_flat, cigar_off=c_off,
+        ref=ref, reads=r_flat, read_off=r_off, anchors=a_flat, anchor_off=a_off,
+        chains=np.array(chain_rows, np.int64),
+        x_score=np.array([x.score for x in results], np.float64),
+        x_span=np.array([[x.read_start, x.read_end, x.ref_start, x.ref_end] for x in results], np.int64),
+        x_counts=np.array([[x.n_match, x.n_mismatch, x.n_insertion, x.n_deletion] for x in results], np.int64),
+        x_cigar=x_flat, x_cigar_off=x_off,
+    )
+    print(f"xdrop_golden.npz: {len(bgrp) - 1} batches ({len(out)} pairs), {len(reads)} reads, "
+          f"{len(results)} chains")
+
+
 if __name__ == "__main__":
     which = sys.argv[1:] or ["sw", "chain", "extend", "hybrid"]
     if "sw" in which:
@@ -631,3 +749,5 @@ if __name__ == "__main__":
         make_seed(np.random.default_rng(505))
     if "wfa" in which:
         make_wfa(np.random.default_rng(606))
+    if "xdrop" in which:
+        make_xdrop(np.random.default_rng(707))

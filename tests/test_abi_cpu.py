@@ -68,7 +68,7 @@ _LAYOUT_C = r"""
 #define P(T) printf(#T " %zu\n", sizeof(T))
 #define O(T, f) printf(#T "." #f " %zu\n", offsetof(T, f))
 int main(void) {
-  P(gmf_pairs); O(gmf_pairs, order); O(gmf_pairs, max_half_band);
+  P(gmf_pairs); O(gmf_pairs, order); O(gmf_pairs, max_half_band); O(gmf_pairs, n_xdrop_groups);
   P(gmf_sw_params); P(gmf_sw_results); O(gmf_sw_results, cigar_capacity); O(gmf_sw_results, error_flags);
   P(gmf_chain_params); O(gmf_chain_params, min_chain_score);
   P(gmf_anchor_batch); O(gmf_anchor_batch, strand);
@@ -92,6 +92,7 @@ def test_ctypes_structs_match_c_layout(tmp_path):
         "gmf_pairs": ctypes.sizeof(n.GmfPairs),
         "gmf_pairs.order": n.GmfPairs.order.offset,
         "gmf_pairs.max_half_band": n.GmfPairs.max_half_band.offset,
+        "gmf_pairs.n_xdrop_groups": n.GmfPairs.n_xdrop_groups.offset,
         "gmf_sw_params": ctypes.sizeof(n.GmfSwParams),
         "gmf_sw_results": ctypes.sizeof(n.GmfSwResults),
         "gmf_sw_results.cigar_capacity": n.GmfSwResults.cigar_capacity.offset,
