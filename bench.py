@@ -60,6 +60,7 @@ def parse():
     p.add_argument("--no-autotune", action="store_true")
     p.add_argument("--long-reads", type=int, default=200,
                    help="reads of the long-read stress leg (2,000 = the full configuration; 0 skips it)")
+    p.add_argument("--wfa-pairs", type=int, default=20_000, help="pairs of the WFA leg (0: skip it)")
     p.add_argument("--serve-loads", default="10000,20000", help="offered loads of the serving leg, reads/s")
     p.add_argument("--serve-requests", type=int, default=600)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -393,6 +394,11 @@ def run_b200(args):
     if args.long_reads > 0:
         longr = long_read_leg(args, device, stream, flush, seed=6 + 1000 * rank, warm=warm)
 
+    # ---- wavefront alignment (the extension's algorithm="wfa" variant) ----
+    wfa_res = None
+    if args.wfa_pairs > 0:
+        wfa_res = wfa_leg(args, device, stream, flush, seed=8 + 1000 * rank, warm=warm)
+
     # ---- serving loop: Poisson requests of 1-64 mixed-profile reads ----
     serve = None
     if not args.no_serve:
@@ -468,9 +474,86 @@ def run_b200(args):
         line["serving"] = serve
     if longr:
         line["long_reads"] = longr
+    if wfa_res:
+        line["wfa"] = wfa_res
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ps, head["params"])
     return line
+
+
+def wfa_leg(args, device, stream, flush, seed: int, warm: int) -> dict:
+    """Wavefront alignment of mixed-length reads against their source stretch
+    (graphmambaformer_b200.wfa): device time of the distance pass alone and of
+    the full alignment (distance pass, history pass, walk), end-to-end time of
+    align_wfa_pairs (host lists in, distances and CIGARs out), and the oracle
+    on a sample of the pairs on the host cores."""
+    import torch
+
+    from graphmambaformer_b200 import synth, wfa
+
+    qs, ts = synth.wfa_pairs_mixed(n_pairs=args.wfa_pairs, seed=seed)
+    md = 4096
+    dp = wfa.upload_wfa_pairs(qs, ts, device)
+    dist = torch.empty(dp.n, dtype=torch.int32, device=device)
+
+    def dstep():
+        wfa.wfa_distances(dp, md, stream, out=dist)
+
+    for _ in range(warm):
+        dstep()
+    torch.cuda.synchronize(device)
+    h_dist = dist.to("cpu").numpy().copy()
+    d_ms = float(np.mean(time_device(dstep, args.steps, stream, flush)))
+
+    def astep():
+        wfa.wfa_distances(dp, md, stream, out=dist)
+        wfa._run_align(dp, dist, h_dist, int(stream.cuda_stream))
+
+    for _ in range(warm):
+        astep()
+    torch.cuda.synchronize(device)
+    a_ms = float(np.mean(time_device(astep, max(2, args.steps // 2), stream, flush)))
+    e = []
+    for _ in range(max(2, args.steps // 4)):
+        t0 = time.perf_counter()
+        r = wfa.align_wfa_pairs(qs, ts, md, device=device)
+        e.append((time.perf_counter() - t0) * 1e3)
+    e_ms = float(np.mean(e))
+    n = len(qs)
+    bases = int(sum(len(q) + len(t) for q, t in zip(qs, ts)))
+    hist = int(np.sum(np.where(h_dist >= 0, (h_dist.astype(np.int64) + 1) ** 2, 0)))
+    out = {
+        "value": n / (a_ms * 1e-3), "unit": "alignments/s", "ms_per_step": a_ms,
+        "bases_per_s": bases / (a_ms * 1e-3),
+        "distance_only": {"value": n / (d_ms * 1e-3), "unit": "alignments/s", "ms_per_step": d_ms},
+        "e2e": {"value": n / (e_ms * 1e-3), "unit": "alignments/s", "ms_per_step": e_ms,
+                "h2d_bytes_per_step": bases + 16 * (n + 1),
+                # distances, op counts, CIGAR starts and lengths, two counters, the CIGAR words
+                "d2h_bytes_per_step": 32 * n + 12 + 4 * int(len(r.cigar_words))},
+        "config": {"workload": "wfa_pairs_mixed", "pairs": n, "read_len": "lognormal(7.0, 1.2) clipped to 150-20000",
+                   "profiles": "Illumina / HiFi / ONT thirds", "target": "the read's source stretch",
+                   "max_distance": md, "bases": bases, "mean_distance": float(h_dist[h_dist >= 0].mean()),
+                   "max_distance_seen": int(h_dist.max()), "history_entries": hist},
+        "gpu_launches_per_step": 3,
+    }
+    if not args.no_cpu_baseline:
+        from oracle import oracle
+
+        rng = np.random.default_rng(1)
+        idx = rng.permutation(n)
+        t0 = time.perf_counter()
+        done, done_bases = 0, 0
+        for b in idx:
+            oracle.wfa_align(qs[b], ts[b], md)
+            done += 1
+            done_bases += len(qs[b]) + len(ts[b])
+            if time.perf_counter() - t0 > 10.0:
+                break
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": done / dt, "unit": "alignments/s", "bases_per_s": done_bases / dt,
+                               "cores": 1, "kind": "port",
+                               "sample": f"{done} random pairs of the workload, oracle_wfa_align, one thread"}
+    return out
 
 
 def long_read_leg(args, device, stream, flush, seed: int, warm: int) -> dict:

@@ -16,14 +16,16 @@
 // diagonal's reach is a run of matches (never negative).
 //
 // Layout:
-//   forward kernel  one warp per pair (persistent warps pull pairs from a
-//                   counter, in the caller's order).  Lanes take the
-//                   diagonals of a wavefront 32 at a time; a lane extends its
-//                   diagonal 4 codes per step (word loads of both sequences
-//                   realigned with a funnel shift, byte compares).  The two
-//                   live wavefronts sit in shared memory while s <= 255 and
-//                   move to the warp's global slot beyond.  With a history
-//                   pointer the warp also stores wavefront s at s*s + s + k.
+//   forward kernel  persistent blocks pull pairs 8 at a time, in the caller's
+//                   order.  A pair is computed by one warp, or by the whole
+//                   block when it is long (a side of 4000 codes in the first
+//                   pass, distance 96 in the second): the team's threads take
+//                   the diagonals of a wavefront in turn and extend each one
+//                   4 codes per step (a sliding window of aligned words of
+//                   both sequences, byte compares).  The two live wavefronts
+//                   sit in shared memory (scores up to 255 for a warp, 2050
+//                   for a block) and move to a global slot beyond.  The
+//                   second pass also stores wavefront s at s*s + s + k.
 //   walk kernel     one thread per pair: two passes over the history (count,
 //                   then write the run-length words back to front).
 
@@ -36,6 +38,9 @@ constexpr int WFA_SMEM_S = 255;                       // wavefronts up to this s
 constexpr int WFA_SMEM_CEN = WFA_SMEM_S + 1;          // index of diagonal 0 in a shared wavefront
 constexpr int WFA_SMEM_WF = 2 * WFA_SMEM_S + 3;       // ints per shared wavefront
 constexpr int WFA_MAX_BLOCKS_PER_SM = 4;
+constexpr int WFA_BLOCK_S = (WFA_WARPS * WFA_SMEM_WF - 3) / 2;  // block-wide wavefronts: scores up to 2050
+constexpr int WFA_LONG_LEN = 4000;  // first pass: a pair with a side this long gets a whole block
+constexpr int WFA_LONG_D = 96;      // second pass: a pair at this distance gets a whole block
 
 struct Seq {
     const uint32_t* w;  // aligned words covering the whole buffer
@@ -82,6 +87,7 @@ struct WfaArgs {
     unsigned long long* hist_used;
     long long* hist_off;   // per pair: offset into hist, -1 when absent
     int* err;
+    int long_len, long_d;  // whole-block pairs: a side of long_len codes (first pass), distance long_d (second)
 };
 
 __device__ __forceinline__ int clip_cand(int v, int k, int n, int m) {
@@ -89,49 +95,88 @@ __device__ __forceinline__ int clip_cand(int v, int k, int n, int m) {
     return (v < 0 || v > n || col < 0 || col > m) ? -1 : v;
 }
 
-// Offset after the run of matches from query position i on diagonal k.
+// Offset after the run of matches from query position i on diagonal k.  Both
+// sequences are read as a sliding window of aligned words (one new word per
+// sequence per 4 codes, loaded one step ahead of the compare).
 __device__ __forceinline__ int wfa_extend(const Seq& Q, long long q0, const Seq& T, long long t0, int n, int m,
                                           int i, int k) {
     if (i < 0) return i;
-    int j = i - k;
-    if (j < 0) return i;
-    while (i < n && j < m) {
-        const unsigned a = Q.get4(q0, i), b = T.get4(t0, j);
+    const int j = i - k;
+    if (j < 0 || i >= n || j >= m) return i;
+    const long long bq = Q.base + q0 + i, bt = T.base + t0 + j;
+    long long wq = bq >> 2, wt = bt >> 2;
+    const int sq = (int)(bq & 3) * 8, st = (int)(bt & 3) * 8;
+    unsigned qa = Q.ld(wq), qb = Q.ld(wq + 1), ta = T.ld(wt), tb = T.ld(wt + 1);
+    const int lim = min(n - i, m - j);
+    int adv = 0;
+    for (;;) {
+        const unsigned qn = Q.ld(wq + 2), tn = T.ld(wt + 2);
+        const unsigned a = __funnelshift_r(qa, qb, sq), b = __funnelshift_r(ta, tb, st);
         const unsigned bad = __vcmpne4(a, b) | __vcmpeq4(a, 0x05050505u) | __vcmpgeu4(a, 0x80808080u);
-        int r = bad ? (__ffs((int)bad) - 1) >> 3 : 4;
-        const int lim = min(n - i, m - j);
-        r = min(r, lim);
-        i += r;
-        j += r;
-        if (r < 4) break;
+        const int r = bad ? (__ffs((int)bad) - 1) >> 3 : 4;
+        adv += r;
+        if (r < 4 || adv >= lim) break;
+        qa = qb;
+        qb = qn;
+        ta = tb;
+        tb = tn;
+        ++wq;
+        ++wt;
     }
-    return i;
+    return i + min(adv, lim);
 }
 
+// A pair is computed by one warp, or by the whole block when it is long.
+struct WarpTeam {
+    int rank;
+    static constexpr int SIZE = 32;
+    __device__ void sync() const { __syncwarp(); }
+    __device__ bool sync_any(bool x) const {
+        __syncwarp();
+        return __any_sync(gmf::FULL_MASK, x);
+    }
+    __device__ long long bcast0(long long v, long long*) const { return __shfl_sync(gmf::FULL_MASK, v, 0); }
+};
+
+struct BlockTeam {
+    int rank;
+    static constexpr int SIZE = WFA_WARPS * 32;
+    __device__ void sync() const { __syncthreads(); }
+    __device__ bool sync_any(bool x) const { return __syncthreads_or(x) != 0; }
+    __device__ long long bcast0(long long v, long long* scratch) const {
+        if (rank == 0) *scratch = v;
+        __syncthreads();
+        const long long r = *scratch;
+        __syncthreads();
+        return r;
+    }
+};
+
 // The wavefronts of one pair up to completion; returns the distance, or -1
-// once `limit` is reached without completing.  With `hist`, wavefront s is
-// also stored at hist[s*s + s + k].
-template <bool HIST>
-__device__ int wfa_forward(const WfaArgs& A, long long q0, long long t0, int n, int m, int limit, int* sm, int* gl,
-                           int* hist, int lane) {
+// once `limit` is reached without completing.  `sm` holds two wavefronts of
+// scores up to `sm_s`; beyond that they move to `gl` (two of 2*eff+3).  With
+// `hist`, wavefront s is also stored at hist[s*s + s + k].
+template <bool HIST, class Team>
+__device__ int wfa_forward(const WfaArgs& A, long long q0, long long t0, int n, int m, int limit, int* sm, int sm_s,
+                           int* gl, int* hist, const Team& tm, long long* scratch) {
     const int final_k = n - m;
-    int h0 = 0;
-    if (lane == 0) h0 = wfa_extend(A.Q, q0, A.T, t0, n, m, 0, 0);
-    h0 = __shfl_sync(gmf::FULL_MASK, h0, 0);
-    if (HIST && lane == 0) hist[0] = h0;
+    long long h0 = 0;
+    if (tm.rank == 0) h0 = wfa_extend(A.Q, q0, A.T, t0, n, m, 0, 0);
+    h0 = tm.bcast0(h0, scratch);
+    if (HIST && tm.rank == 0) hist[0] = (int)h0;
     if (final_k == 0 && h0 >= n) return 0;
     int* prev = sm;
-    int* cur = sm + WFA_SMEM_WF;
-    int cen = WFA_SMEM_CEN;
-    if (lane == 0) prev[cen] = h0;
-    __syncwarp();
+    int* cur = sm + 2 * sm_s + 3;
+    int cen = sm_s + 1;
+    if (tm.rank == 0) prev[cen] = (int)h0;
+    tm.sync();
     bool shared = true;
     for (int s = 1;; ++s) {
         if (s - 1 >= limit || s > A.eff) return -1;  // s <= max(n, m) <= eff always holds
-        if (shared && s > WFA_SMEM_S) {  // move the live wavefront to the global slot
+        if (shared && s > sm_s) {  // move the live wavefront to the global slot
             const int gcen = A.eff + 1;
-            for (int k = -(s - 1) + lane; k <= s - 1; k += 32) gl[k + gcen] = prev[k + cen];
-            __syncwarp();
+            for (int k = -(s - 1) + tm.rank; k <= s - 1; k += Team::SIZE) gl[k + gcen] = prev[k + cen];
+            tm.sync();
             prev = gl;
             cur = gl + 2 * A.eff + 3;
             cen = gcen;
@@ -139,8 +184,8 @@ __device__ int wfa_forward(const WfaArgs& A, long long q0, long long t0, int n, 
         }
         const int ps = s - 1;
         bool done = false;
-        for (int base = -s; base <= s; base += 32) {
-            const int k = base + lane;
+        for (int base = -s; base <= s; base += Team::SIZE) {
+            const int k = base + tm.rank;
             if (k <= s) {
                 int sub = (k >= -ps && k <= ps) ? prev[k + cen] : -1;
                 int ins = (k - 1 >= -ps && k - 1 <= ps) ? prev[k - 1 + cen] : -1;
@@ -155,59 +200,103 @@ __device__ int wfa_forward(const WfaArgs& A, long long q0, long long t0, int n, 
                 done |= (k == final_k) && r >= n;
             }
         }
-        __syncwarp();
-        if (__any_sync(gmf::FULL_MASK, done)) return s;
+        if (tm.sync_any(done)) return s;
         int* tmp = prev;
         prev = cur;
         cur = tmp;
     }
 }
 
+// One pair: its distance (first pass) or its history (second pass).
+template <bool HIST, class Team>
+__device__ void wfa_pair(const WfaArgs& A, int p, int* sm, int sm_s, int* gl, const Team& tm, long long* scratch) {
+    const long long q0 = A.q_off[p], t0 = A.t_off[p];
+    const int n = (int)(A.q_off[p + 1] - q0), m = (int)(A.t_off[p + 1] - t0);
+    if (!HIST) {
+        int d;
+        if (n == 0 || m == 0)
+            d = max(n, m);
+        else
+            d = wfa_forward<false>(A, q0, t0, n, m, A.max_distance, sm, sm_s, gl, nullptr, tm, scratch);
+        if (tm.rank == 0) A.distance[p] = d;
+        return;
+    }
+    const int d = A.distance[p];
+    long long off = -1;
+    if (d > A.eff) {
+        if (tm.rank == 0) atomicOr(A.err, (int)GMF_SWF_WORKSPACE);
+    } else if (d >= 0 && n > 0 && m > 0) {
+        const long long need = (long long)(d + 1) * (d + 1);
+        if (tm.rank == 0) {
+            const unsigned long long o = atomicAdd(A.hist_used, (unsigned long long)need);
+            if ((long long)o + need <= A.hist_cap)
+                off = (long long)o;
+            else
+                atomicOr(A.err, (int)GMF_SWF_WORKSPACE);
+        }
+        off = tm.bcast0(off, scratch);
+        if (off >= 0) {
+            const int got = wfa_forward<true>(A, q0, t0, n, m, d, sm, sm_s, gl, A.hist + off, tm, scratch);
+            if (got != d) off = -1;  // cannot happen: the pass is deterministic
+        }
+    }
+    if (tm.rank == 0) A.hist_off[p] = off;
+}
+
+__device__ __forceinline__ bool wfa_is_long(const WfaArgs& A, int p, bool hist) {
+    if (hist) return A.distance[p] >= A.long_d;
+    const long long n = A.q_off[p + 1] - A.q_off[p], m = A.t_off[p + 1] - A.t_off[p];
+    return (n > m ? n : m) >= A.long_len;
+}
+
+// Blocks pull positions of the caller's order.  A block takes one position
+// and, when its pair is long, computes it with all its warps (wavefronts in
+// the block's shared memory up to score 2050); otherwise it takes 7 more
+// positions and its warps compute one pair each (a long pair among those
+// goes first, block-wide).  With a longest-first order every long pair gets a
+// block of its own.
 template <bool HIST>
 __global__ void __launch_bounds__(WFA_WARPS * 32) wfa_forward_kernel(WfaArgs A) {
-    __shared__ int s_wf[WFA_WARPS][2 * WFA_SMEM_WF];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const long long gw = (long long)blockIdx.x * WFA_WARPS + wib;
-    int* gl = A.spill ? A.spill + gw * 2 * (2ll * A.eff + 3) : nullptr;
+    __shared__ int s_wf[WFA_WARPS * 2 * WFA_SMEM_WF];
+    __shared__ int s_pos[WFA_WARPS];
+    __shared__ long long s_scratch;
+    const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
+    const long long slot = 2 * (2ll * A.eff + 3);
+    int* gl_warp = A.spill ? A.spill + ((long long)blockIdx.x * WFA_WARPS + wib) * slot : nullptr;
+    int* gl_block = A.spill ? A.spill + (long long)blockIdx.x * WFA_WARPS * slot : nullptr;
+    const unsigned n = (unsigned)A.n_pairs;
     for (;;) {
-        unsigned idx = 0;
-        if (lane == 0) idx = atomicAdd(A.work, 1u);
-        idx = __shfl_sync(gmf::FULL_MASK, idx, 0);
-        if (idx >= (unsigned)A.n_pairs) break;
-        const int p = A.order ? A.order[idx] : (int)idx;
-        const long long q0 = A.q_off[p], t0 = A.t_off[p];
-        const int n = (int)(A.q_off[p + 1] - q0), m = (int)(A.t_off[p + 1] - t0);
-        if (!HIST) {
-            int d;
-            if (n == 0 || m == 0)
-                d = max(n, m);
-            else
-                d = wfa_forward<false>(A, q0, t0, n, m, A.max_distance, s_wf[wib], gl, nullptr, lane);
-            if (lane == 0) A.distance[p] = d;
-        } else {
-            const int d = A.distance[p];
-            long long off = -1;
-            if (d > A.eff) {
-                if (lane == 0) atomicOr(A.err, (int)GMF_SWF_WORKSPACE);
-            } else if (d >= 0 && n > 0 && m > 0) {
-                const long long need = (long long)(d + 1) * (d + 1);
-                if (lane == 0) {
-                    const unsigned long long o = atomicAdd(A.hist_used, (unsigned long long)need);
-                    if ((long long)o + need <= A.hist_cap) {
-                        off = (long long)o;
-                    } else {
-                        atomicOr(A.err, (int)GMF_SWF_WORKSPACE);
-                    }
-                }
-                off = __shfl_sync(gmf::FULL_MASK, off, 0);
-                if (off >= 0) {
-                    const int got = wfa_forward<true>(A, q0, t0, n, m, d, s_wf[wib], gl, A.hist + off, lane);
-                    if (got != d) off = -1;  // cannot happen: the pass is deterministic
+        if (tid == 0) {
+            const unsigned first = atomicAdd(A.work, 1u);
+            s_pos[0] = first < n ? (int)first : -1;
+            for (int e = 1; e < WFA_WARPS; ++e) s_pos[e] = -1;
+            if (first < n) {
+                const int p = A.order ? A.order[first] : (int)first;
+                if (!wfa_is_long(A, p, HIST)) {
+                    const unsigned more = atomicAdd(A.work, (unsigned)(WFA_WARPS - 1));
+                    for (int e = 1; e < WFA_WARPS; ++e)
+                        if (more + e - 1 < n) s_pos[e] = (int)(more + e - 1);
                 }
             }
-            if (lane == 0) A.hist_off[p] = off;
         }
-        __syncwarp();
+        __syncthreads();
+        if (s_pos[0] < 0) break;
+        bool any_long = false;
+        for (int e = 0; e < WFA_WARPS; ++e) {
+            if (s_pos[e] < 0) continue;
+            const int p = A.order ? A.order[s_pos[e]] : s_pos[e];
+            if (wfa_is_long(A, p, HIST)) {
+                wfa_pair<HIST>(A, p, s_wf, WFA_BLOCK_S, gl_block, BlockTeam{tid}, &s_scratch);
+                any_long = true;
+            }
+        }
+        if (any_long) __syncthreads();
+        if (s_pos[wib] >= 0) {
+            const int p = A.order ? A.order[s_pos[wib]] : s_pos[wib];
+            if (!wfa_is_long(A, p, HIST))
+                wfa_pair<HIST>(A, p, s_wf + wib * 2 * WFA_SMEM_WF, WFA_SMEM_S, gl_warp, WarpTeam{lane}, nullptr);
+        }
+        __syncthreads();
     }
 }
 
@@ -427,6 +516,8 @@ WfaArgs base_args(const gmf_wfa_pairs* pairs, int32_t max_distance, int eff, con
     a.work = w.work;
     a.hist_used = w.hist_used;
     a.hist_off = w.hist_off;
+    a.long_len = WFA_LONG_LEN;
+    a.long_d = WFA_LONG_D;
     return a;
 }
 

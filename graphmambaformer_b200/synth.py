@@ -242,6 +242,17 @@ def extension_pairs_mixed(n_pairs: int = 100_000, seed: int = 3, ref_len: int = 
                                         band_slope=band_slope, ref_len=ref_len))
 
 
+def wfa_pairs_mixed(n_pairs: int = 20_000, seed: int = 8, flank: int = 32, **kw) -> tuple:
+    """End-to-end pairs for the wavefront aligner: the mixed-length reads of
+    :func:`extension_pairs_mixed` against the reference stretch they came from
+    (the window the WFA extension takes from an exact chain: no flanks).
+    Returns (queries, targets) lists of int8 codes."""
+    ps = extension_pairs_mixed(n_pairs=n_pairs, seed=seed, flank=flank, **kw)
+    qs = [ps.q(b) for b in range(len(ps))]
+    ts = [ps.t(b)[flank: len(ps.t(b)) - flank] for b in range(len(ps))]
+    return qs, ts
+
+
 # --------------------------------------------------------------------------- #
 # Minimizer sketch (host side, used to produce chaining anchors)
 # --------------------------------------------------------------------------- #
