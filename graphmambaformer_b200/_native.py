@@ -168,6 +168,37 @@ class GmfWfaResults(Structure):
     ]
 
 
+class GmfHostPairs(Structure):
+    _fields_ = [
+        ("n_pairs", c_int32),
+        ("query", c_void_p),
+        ("query_off", c_void_p),
+        ("target", c_void_p),
+        ("target_off", c_void_p),
+        ("half_band", c_void_p),
+        ("band_offset", c_void_p),
+        ("xdrop_group_off", c_void_p),
+        ("n_xdrop_groups", c_int32),
+    ]
+
+
+class GmfHostSwResults(Structure):
+    _fields_ = [
+        ("score", c_void_p),
+        ("query_end", c_void_p),
+        ("target_end", c_void_p),
+        ("query_start", c_void_p),
+        ("target_start", c_void_p),
+        ("op_counts", c_void_p),
+        ("cigar", c_void_p),
+        ("cigar_capacity", c_int64),
+        ("cigar_start", c_void_p),
+        ("cigar_len", c_void_p),
+        ("cigar_used", c_void_p),
+        ("error_flags", c_void_p),
+    ]
+
+
 MAX_WFA_DISTANCE = 1 << 16
 
 # name -> (restype, argtypes)
@@ -198,6 +229,12 @@ _SIGNATURES = {
                                 POINTER(GmfChainResults), c_void_p, c_size_t, c_void_p]),
     "gmf_chain_batch_noalloc": (c_int, [POINTER(GmfAnchorBatch), POINTER(GmfChainParams), c_void_p,
                                         c_int32, c_int64, POINTER(GmfChainResults), c_void_p]),
+    "gmf_ctx_create": (c_int, [c_int, c_int32, c_size_t, POINTER(c_void_p)]),
+    "gmf_ctx_destroy": (c_int, [c_void_p]),
+    "gmf_batch_submit": (c_int, [c_void_p, POINTER(GmfHostPairs), POINTER(GmfSwParams), POINTER(GmfHostSwResults),
+                                 POINTER(c_int64)]),
+    "gmf_batch_poll": (c_int, [c_void_p, c_int64]),
+    "gmf_batch_wait": (c_int, [c_void_p, c_int64]),
     "gmf_wfa_workspace_bytes": (c_size_t, [c_int32, c_int32, c_int32, c_int64]),
     "gmf_wfa_history_entries": (c_int64, [c_int32, c_void_p, c_void_p, c_void_p]),
     "gmf_wfa_distance": (c_int, [POINTER(GmfWfaPairs), c_int32, c_void_p, c_void_p, c_size_t, c_void_p]),

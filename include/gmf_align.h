@@ -26,6 +26,9 @@
  *   gmf_chain_sort    alignment/types.py L144-152 (for_strand, sorted_by_ref)
  *   gmf_chain_batch   alignment/chaining.py L620-745 (AffineChainer.chain /
  *                     chain_batch: sort, DP, _backtrack, select)
+ *   gmf_ctx_*, gmf_batch_*  the asynchronous serving form of gmf_banded_sw on
+ *                     host buffers (the reference has none: its wrappers run
+ *                     synchronously on the caller's tensors)
  *   gmf_wfa_distance  accel/cuda_kernels.py L569-600 (wfa_distance)
  *   gmf_wfa_align     alignment/extension.py L308-463 (WavefrontAligner)
  */
@@ -338,6 +341,70 @@ int gmf_chain_batch(const gmf_anchor_batch* anchors, const gmf_chain_params* par
 int gmf_chain_batch_noalloc(const gmf_anchor_batch* anchors, const gmf_chain_params* params,
                             const double* pen_lut, int32_t lut_len, int64_t n_anchors,
                             const gmf_chain_results* results, gmf_stream_t stream);
+
+/* ======================================================================== */
+/* Contexts and asynchronous batches on HOST buffers                        */
+/* ======================================================================== */
+
+/* A context owns, on one device, `slots` (1..8) slots of a stream, pinned
+ * staging memory and a device arena (inputs, outputs and workspace of one
+ * batch): up to `slots` batches in flight.  A slot may hold up to
+ * memory_budget / slots bytes of device memory (memory_budget 0 = no limit);
+ * its arena grows, never shrinks.  One context serves any number of threads
+ * (calls are serialised inside). */
+typedef struct gmf_ctx gmf_ctx;
+
+int gmf_ctx_create(int device, int32_t slots, size_t memory_budget, gmf_ctx** ctx);
+int gmf_ctx_destroy(gmf_ctx* ctx); /* waits for the batches in flight */
+
+/* A batch in HOST memory, read only during gmf_batch_submit (fields as in
+ * gmf_pairs; the processing order is chosen inside). */
+typedef struct {
+    int32_t n_pairs;
+    const int8_t* query;
+    const int64_t* query_off;  /* n_pairs+1, from 0 */
+    const int8_t* target;
+    const int64_t* target_off; /* n_pairs+1, from 0 */
+    const int32_t* half_band;
+    const int32_t* band_offset;
+    const int32_t* xdrop_group_off; /* optional, as in gmf_pairs */
+    int32_t n_xdrop_groups;
+} gmf_host_pairs;
+
+/* HOST outputs (layout as in gmf_sw_results), written when the batch
+ * completes: gmf_batch_poll returns GMF_OK, or gmf_batch_wait returns. */
+typedef struct {
+    int32_t* score;
+    int32_t* query_end;
+    int32_t* target_end;
+    int32_t* query_start;      /* with cigar */
+    int32_t* target_start;     /* with cigar */
+    int32_t* op_counts;        /* 4 per pair or NULL */
+    uint32_t* cigar;           /* NULL = score and ends only */
+    int64_t cigar_capacity;    /* words */
+    int64_t* cigar_start;      /* with cigar */
+    int32_t* cigar_len;        /* with cigar */
+    int64_t* cigar_used;       /* words written */
+    int32_t* error_flags;      /* GMF_SWF_* of the batch */
+} gmf_host_sw_results;
+
+/* Enqueue one batch of gmf_banded_sw: the inputs go to the device in one
+ * copy, the kernels run on the slot's stream and the fixed-size outputs come
+ * back in one copy, all asynchronously.  Slots are taken in turn; when the
+ * next one still holds a batch, that batch is completed first (its outputs
+ * written; its ticket then reports GMF_OK once).  GMF_ERR_LIMIT when the
+ * batch needs more than a slot's share of the budget.  *ticket identifies the
+ * batch. */
+int gmf_batch_submit(gmf_ctx* ctx, const gmf_host_pairs* pairs, const gmf_sw_params* params,
+                     const gmf_host_sw_results* results, int64_t* ticket);
+
+/* GMF_OK once the batch is complete and its outputs written (reported once
+ * per ticket), GMF_ERR_NOT_READY while it is in flight,
+ * GMF_ERR_INVALID_ARGUMENT for an unknown ticket. */
+int gmf_batch_poll(gmf_ctx* ctx, int64_t ticket);
+
+/* As gmf_batch_poll, blocking until the batch completes. */
+int gmf_batch_wait(gmf_ctx* ctx, int64_t ticket);
 
 /* ======================================================================== */
 /* Unit-cost global wavefront alignment (WFA)                               */

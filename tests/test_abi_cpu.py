@@ -75,6 +75,8 @@ int main(void) {
   P(gmf_sorted_anchors); P(gmf_chain_results); O(gmf_chain_results, members);
   P(gmf_wfa_pairs); O(gmf_wfa_pairs, query_total); O(gmf_wfa_pairs, max_len);
   P(gmf_wfa_results); O(gmf_wfa_results, cigar_capacity); O(gmf_wfa_results, error_flags);
+  P(gmf_host_pairs); O(gmf_host_pairs, n_xdrop_groups);
+  P(gmf_host_sw_results); O(gmf_host_sw_results, cigar_capacity); O(gmf_host_sw_results, error_flags);
   return 0;
 }
 """
@@ -110,6 +112,11 @@ def test_ctypes_structs_match_c_layout(tmp_path):
         "gmf_wfa_results": ctypes.sizeof(n.GmfWfaResults),
         "gmf_wfa_results.cigar_capacity": n.GmfWfaResults.cigar_capacity.offset,
         "gmf_wfa_results.error_flags": n.GmfWfaResults.error_flags.offset,
+        "gmf_host_pairs": ctypes.sizeof(n.GmfHostPairs),
+        "gmf_host_pairs.n_xdrop_groups": n.GmfHostPairs.n_xdrop_groups.offset,
+        "gmf_host_sw_results": ctypes.sizeof(n.GmfHostSwResults),
+        "gmf_host_sw_results.cigar_capacity": n.GmfHostSwResults.cigar_capacity.offset,
+        "gmf_host_sw_results.error_flags": n.GmfHostSwResults.error_flags.offset,
     }
     for k, v in want.items():
         assert int(got[k]) == v, (k, got[k], v)
@@ -168,3 +175,12 @@ def test_entry_points_reject_malformed_arguments_before_any_cuda_call():
     p = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
     assert lib.gmf_wfa_history_entries(3, p(ql), p(tl), p(dist)) == 16
     assert lib.gmf_wfa_workspace_bytes(3, 12, 8, 16) >= lib.gmf_wfa_workspace_bytes(3, 12, 8, 0) + 64
+    # contexts: malformed calls are refused before any CUDA call
+    assert lib.gmf_ctx_create(0, 3, 0, None) == _native.GMF_ERR_INVALID_ARGUMENT
+    h = ctypes.c_void_p()
+    assert lib.gmf_ctx_create(0, 0, 0, ctypes.byref(h)) == _native.GMF_ERR_INVALID_ARGUMENT
+    assert lib.gmf_ctx_create(0, 9, 0, ctypes.byref(h)) == _native.GMF_ERR_INVALID_ARGUMENT
+    assert lib.gmf_ctx_destroy(None) == _native.GMF_ERR_INVALID_ARGUMENT
+    assert lib.gmf_batch_submit(None, None, None, None, None) == _native.GMF_ERR_INVALID_ARGUMENT
+    assert lib.gmf_batch_poll(None, 1) == _native.GMF_ERR_INVALID_ARGUMENT
+    assert lib.gmf_batch_wait(None, 1) == _native.GMF_ERR_INVALID_ARGUMENT
