@@ -199,6 +199,32 @@ class GmfHostSwResults(Structure):
     ]
 
 
+class GmfSamRecords(Structure):
+    _fields_ = [
+        ("n_records", c_int32),
+        ("name", c_void_p),
+        ("name_off", c_void_p),
+        ("seq", c_void_p),
+        ("seq_off", c_void_p),
+        ("qual", c_void_p),
+        ("contig", c_void_p),
+        ("contig_names", c_void_p),
+        ("contig_off", c_void_p),
+        ("n_contigs", c_int32),
+        ("ref_start", c_void_p),
+        ("ref_end", c_void_p),
+        ("strand", c_void_p),
+        ("mapq", c_void_p),
+        ("cigar", c_void_p),
+        ("cigar_start", c_void_p),
+        ("cigar_len", c_void_p),
+        ("clip_left", c_void_p),
+        ("clip_right", c_void_p),
+        ("tags", c_void_p),
+        ("tag_off", c_void_p),
+    ]
+
+
 MAX_WFA_DISTANCE = 1 << 16
 
 # name -> (restype, argtypes)
@@ -235,6 +261,8 @@ _SIGNATURES = {
                                  POINTER(c_int64)]),
     "gmf_batch_poll": (c_int, [c_void_p, c_int64]),
     "gmf_batch_wait": (c_int, [c_void_p, c_int64]),
+    "gmf_sam_count": (c_int, [POINTER(GmfSamRecords), c_void_p, c_void_p]),
+    "gmf_sam_fill": (c_int, [POINTER(GmfSamRecords), c_void_p, c_void_p, c_void_p]),
     "gmf_wfa_workspace_bytes": (c_size_t, [c_int32, c_int32, c_int32, c_int64]),
     "gmf_wfa_history_entries": (c_int64, [c_int32, c_void_p, c_void_p, c_void_p]),
     "gmf_wfa_distance": (c_int, [POINTER(GmfWfaPairs), c_int32, c_void_p, c_void_p, c_size_t, c_void_p]),

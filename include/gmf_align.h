@@ -29,6 +29,7 @@
  *   gmf_ctx_*, gmf_batch_*  the asynchronous serving form of gmf_banded_sw on
  *                     host buffers (the reference has none: its wrappers run
  *                     synchronously on the caller's tensors)
+ *   gmf_sam_count/fill  data/formats.py L343-397 + L476-500 (SAM records)
  *   gmf_wfa_distance  accel/cuda_kernels.py L569-600 (wfa_distance)
  *   gmf_wfa_align     alignment/extension.py L308-463 (WavefrontAligner)
  */
@@ -405,6 +406,49 @@ int gmf_batch_poll(gmf_ctx* ctx, int64_t ticket);
 
 /* As gmf_batch_poll, blocking until the batch completes. */
 int gmf_batch_wait(gmf_ctx* ctx, int64_t ticket);
+
+/* ======================================================================== */
+/* SAM text of alignment records                                            */
+/* ======================================================================== */
+
+/* Records to render as SAM lines (all device arrays; offsets from 0).  A
+ * record is mapped when contig >= 0, it has bases, ref_end > ref_start and a
+ * non-empty CIGAR; then, as the reference writes it, strand -1 reorients it
+ * (FLAG 0x10, CIGAR runs reversed, SEQ reverse-complemented, QUAL reversed),
+ * and a CIGAR whose query length (= X I S M) differs from the number of bases
+ * makes it unmapped after all.  Unmapped: FLAG 0x4, RNAME '*', POS 0, MAPQ 0,
+ * CIGAR '*'.  Columns 7-9 are '*', 0, 0 (single-end). */
+typedef struct {
+    int32_t n_records;
+    const char* name;            /* QNAME bytes */
+    const int64_t* name_off;     /* n_records+1 */
+    const char* seq;             /* bases as given (ASCII) */
+    const int64_t* seq_off;      /* n_records+1 */
+    const uint8_t* qual;         /* Phred value per base (seq_off layout), NULL = all 0; clamped to 93 */
+    const int32_t* contig;       /* per record: contig index, -1 = no alignment */
+    const char* contig_names;    /* RNAME bytes of each contig */
+    const int64_t* contig_off;   /* n_contigs+1 */
+    int32_t n_contigs;
+    const int64_t* ref_start;    /* 0-based */
+    const int64_t* ref_end;
+    const int8_t* strand;        /* +1 / -1 */
+    const int32_t* mapq;
+    const uint32_t* cigar;       /* words (run << 4) | op: 0 '=', 1 'X', 2 'I', 3 'D', 4 'S', 5 'M', 6 'N', 7 'H' */
+    const int64_t* cigar_start;  /* per record */
+    const int32_t* cigar_len;    /* per record, words */
+    const int32_t* clip_left;    /* optional soft clips around the words (NULL = none), merged with an */
+    const int32_t* clip_right;   /* adjacent S word */
+    const char* tags;            /* optional tag text per record (tab-separated fields), NULL = none */
+    const int64_t* tag_off;      /* n_records+1 with tags */
+} gmf_sam_records;
+
+/* Length in bytes of every record's line (newline included). */
+int gmf_sam_count(const gmf_sam_records* records, int64_t* line_len, gmf_stream_t stream);
+
+/* Write every record's line at text + line_off[r] (the exclusive scan of the
+ * lengths).  Replaces data/formats.py L343-397 (_make_segment) and the SAM
+ * rendering of write_sam (L476-500) for single-end records. */
+int gmf_sam_fill(const gmf_sam_records* records, const int64_t* line_off, char* text, gmf_stream_t stream);
 
 /* ======================================================================== */
 /* Unit-cost global wavefront alignment (WFA)                               */

@@ -39,6 +39,14 @@ Fixtures:
   batches whose members drop on different rows (small ``x_drop``), and
   ``extend_chains`` on reads with unalignable blocks next to secondary
   chains, where a chain keeps extending while another has not dropped.
+* ``sam_golden.pkl``    -- record assembly and SAM fields: the pipeline's
+  ``_margin_mapq`` and ``_records`` on ``extend_chains`` results (both
+  algorithms, both strands, reads without chains), then
+  ``alignments_to_records`` and the field assignments of ``_make_segment``
+  (data/formats.py L343-397) captured on a stand-in segment object, since
+  pysam is not installed here.  Edge records cover a CIGAR that does not
+  match the read, an empty span, qualities out of range or short, bases
+  outside ACGTN and contig-name overrides.
 * ``hybrid_golden.pkl`` -- ``AffineChainer.chain`` with a ``ChainingContext``
   (graph-distance oracle, backbone bias, neural seed scores with each AGNES
   trust decision, learned transitions).
@@ -735,6 +743,153 @@ def make_xdrop(rng):
           f"{len(results)} chains")
 
 
+# --------------------------------------------------------------------------- #
+# record assembly + SAM segment fields
+# --------------------------------------------------------------------------- #
+class _Segment:
+    """Stand-in for pysam.AlignedSegment: keeps every field assigned."""
+
+    def __init__(self):
+        self.query_name = None
+        self.flag = 0
+        self.reference_id = -1
+        self.reference_start = -1
+        self.mapping_quality = 255
+        self.cigartuples = None
+        self.next_reference_id = -1
+        self.next_reference_start = -1
+        self.template_length = 0
+        self.query_sequence = None
+        self.query_qualities = None
+        self.tags = []
+
+    def set_tag(self, key, value):
+        self.tags.append((key, value))
+
+
+class _Pysam:
+    AlignedSegment = _Segment
+
+
+def make_sam(rng):
+    import pickle
+    from types import SimpleNamespace
+
+    from graphmambaformer.alignment.pipeline import AlignmentPipeline
+    from graphmambaformer.alignment.seeding import SeedIndexBundle
+    from graphmambaformer.alignment.types import AlignmentRecord, ReadAlignments
+    from graphmambaformer.data import alignment_io, formats
+
+    ref = synth.random_reference(300_000, rng)
+    ref_str = synth.decode_bases(ref)
+    bundle = object.__new__(SeedIndexBundle)
+    bundle.node_starts = np.arange(0, len(ref), 1000, dtype=np.int64)
+    bundle.node_ids = np.arange(len(bundle.node_starts), dtype=np.int64) * 3 + 7
+    reference = SimpleNamespace(ref_id=0, bundle=bundle)
+    stub = SimpleNamespace(uses_neural_scoring=False, mode="fast",
+                           cfg=SimpleNamespace(scoring=SimpleNamespace(max_mapq=60)))
+    profiles = (synth.ILLUMINA, synth.HIFI, synth.ONT)
+    modalities = ("illumina", "pacbio_hifi", "ont")
+    reads_in, results, calls = [], [], []
+    for r in range(36):
+        algo = r % 2
+        prof = profiles[(r // 2) % 3]
+        L = int(rng.integers(80, 1500))
+        s0 = int(rng.integers(500, len(ref) - L - 500))
+        strand = 1 if (r // 4) % 2 == 0 else -1
+        tmpl = ref[s0: s0 + L]
+        read = synth.apply_errors(tmpl if strand > 0 else synth.reverse_complement(tmpl), prof, rng)
+        seq = synth.decode_bases(read)
+        if r % 9 == 4:  # bases outside ACGTN ride along in SEQ
+            seq = seq[:10] + "R" + seq[11:20] + "a" + seq[21:]
+        oriented = read if strand > 0 else synth.reverse_complement(read)
+        n = len(oriented)
+        rp_l, fp_l, rows = [], [], []
+        n_chains = 0 if r % 7 == 6 else int(rng.integers(1, 4))
+        for c in range(n_chains):
+            k = int(rng.integers(2, 5))
+            rp = np.sort(rng.choice(np.arange(0, max(n - 20, 1)), size=min(k, max(n - 20, 1)), replace=False))
+            if c == 0:
+                fp = s0 + rp + rng.integers(-3, 4, size=len(rp))
+                cs = strand
+            else:
+                base = int(rng.integers(1000, len(ref) - n - 1000))
+                fp = base + rp + rng.integers(-30, 31, size=len(rp))
+                cs = strand if rng.random() < 0.5 else -strand
+            lo = sum(len(x) for x in rp_l)
+            rp_l.append(rp.astype(np.int64))
+            fp_l.append(fp.astype(np.int64))
+            rows.append((lo, lo + len(rp), cs))
+        rpa = np.concatenate(rp_l) if rp_l else np.zeros(0, np.int64)
+        fpa = np.concatenate(fp_l) if fp_l else np.zeros(0, np.int64)
+        ln = np.full(len(rpa), 15, np.int64)
+        st = np.concatenate([np.full(hi - lo, cs, np.int8) for lo, hi, cs in rows]) if rows else np.zeros(0, np.int8)
+        anchors = AnchorSet.from_lists(rpa, fpa, ln, st)
+        chains = [Chain(anchor_idx=np.arange(lo, hi), score=float(rng.integers(20, 400)), strand=cs,
+                        read_start=int(rpa[lo:hi].min()), read_end=int((rpa[lo:hi] + 15).max()),
+                        ref_start=int(fpa[lo:hi].min()), ref_end=int((fpa[lo:hi] + 15).max()),
+                        is_primary=(c == 0))
+                  for c, (lo, hi, cs) in enumerate(rows)]
+        cfg = ExtensionConfig(algorithm="wfa" if algo else "banded_sw")
+        eng = ExtensionEngine(cfg, device="cpu", backend="torch")
+        exts = eng.extend_chains(seq, chains, anchors, ref_str) if chains else []
+        if r % 11 == 3 and exts:
+            exts = exts[:1]  # fewer extensions than chains: the rest keep chain spans, no CIGAR
+        rid = f"read{r}/{L}"
+        mapq = AlignmentPipeline._margin_mapq(stub, chains)
+        records = AlignmentPipeline._records(stub, rid, len(seq), anchors, chains, exts, reference, mapq=mapq,
+                                             route="fast")
+        records = records or [AlignmentRecord.unmapped(rid, len(seq), pass_name="fast")]
+        if r % 13 == 5:  # a record whose CIGAR does not cover the read, and one with an empty span
+            records.append(AlignmentRecord(read_id=rid, read_len=len(seq), ref_id=0, ref_start=100, ref_end=160,
+                                           strand=-1, mapq=7, cigar=[("=", 5)], is_mapped=True,
+                                           is_primary=False))
+            records.append(AlignmentRecord(read_id=rid, read_len=len(seq), ref_id=0, ref_start=100, ref_end=100,
+                                           strand=1, mapq=7, cigar=[("=", len(seq))], is_mapped=True,
+                                           is_primary=False))
+        res = ReadAlignments(read_id=rid, read_len=len(seq), anchors=anchors, chains=list(chains), records=records)
+        quals = None
+        if r % 3 == 1:
+            quals = [int(q) for q in rng.integers(-5, 120, size=len(seq) - (7 if r % 6 == 1 else 0))]
+        src = seq if quals is None and r % 4 == 0 else SimpleNamespace(read_id=rid, seq=seq, quals=quals,
+                                                                       modality=modalities[(r // 2) % 3])
+        reads_in.append(src)
+        results.append(res)
+        calls.append(dict(read_id=rid, seq=seq, quals=quals, modality=None if isinstance(src, str) else src.modality,
+                          anchors=np.stack([rpa, fpa, ln, st.astype(np.int64)], 1) if len(rpa) else np.zeros((0, 4),
+                                                                                                        np.int64),
+                          chains=[(lo, hi, cs, ch.score, ch.is_primary) for (lo, hi, cs), ch in zip(rows, chains)],
+                          algo=algo, n_ext=len(exts), mapq=mapq,
+                          ext=[dict(score=e.score, cigar=list(e.cigar), read_start=e.read_start, read_end=e.read_end,
+                                    ref_start=e.ref_start, ref_end=e.ref_end,
+                                    counts=(e.n_match, e.n_mismatch, e.n_insertion, e.n_deletion)) for e in exts],
+                          records=[dict(vars(x), extension=None) for x in records]))
+    out = {}
+    refs = {0: SimpleNamespace(seq=ref_str)}
+    for inc in (False, True):
+        for names in (None, {0: "chr21"}):
+            recs = alignment_io.alignments_to_records(results, reads_in, modality="pacbio_hifi",
+                                                      include_secondary=inc)
+            sq, ref_index = formats._sq_from_references(refs, names)
+            segs = []
+            for rec in recs:
+                a = formats._make_segment(_Pysam, rec, ref_index)
+                segs.append(dict(qname=a.query_name, flag=a.flag, ref=a.reference_id, pos=a.reference_start,
+                                 mapq=a.mapping_quality, cigar=a.cigartuples, seq=a.query_sequence,
+                                 qual=None if a.query_qualities is None else list(a.query_qualities),
+                                 tags=list(a.tags), rnext=a.next_reference_id, pnext=a.next_reference_start,
+                                 tlen=a.template_length))
+            out[(inc, None if names is None else "chr21")] = dict(sq=sq, segments=segs)
+    payload = dict(ref=ref, node_starts=bundle.node_starts, node_ids=bundle.node_ids, calls=calls, outputs=out,
+                   header_rg=[formats._rg_from_records(alignment_io.alignments_to_records(
+                       results, reads_in, modality="pacbio_hifi", include_secondary=True))])
+    with open(os.path.join(HERE, "sam_golden.pkl"), "wb") as fh:
+        pickle.dump(payload, fh, protocol=4)
+    print(f"sam_golden.pkl: {len(calls)} reads, "
+          f"{sum(len(c['records']) for c in calls)} records, "
+          f"{len(out[(True, None)]['segments'])} segments with secondaries")
+
+
 if __name__ == "__main__":
     which = sys.argv[1:] or ["sw", "chain", "extend", "hybrid"]
     if "sw" in which:
@@ -751,3 +906,5 @@ if __name__ == "__main__":
         make_wfa(np.random.default_rng(606))
     if "xdrop" in which:
         make_xdrop(np.random.default_rng(707))
+    if "sam" in which:
+        make_sam(np.random.default_rng(808))

@@ -76,6 +76,7 @@ int main(void) {
   P(gmf_wfa_pairs); O(gmf_wfa_pairs, query_total); O(gmf_wfa_pairs, max_len);
   P(gmf_wfa_results); O(gmf_wfa_results, cigar_capacity); O(gmf_wfa_results, error_flags);
   P(gmf_host_pairs); O(gmf_host_pairs, n_xdrop_groups);
+  P(gmf_sam_records); O(gmf_sam_records, n_contigs); O(gmf_sam_records, tag_off);
   P(gmf_host_sw_results); O(gmf_host_sw_results, cigar_capacity); O(gmf_host_sw_results, error_flags);
   return 0;
 }
@@ -112,6 +113,9 @@ def test_ctypes_structs_match_c_layout(tmp_path):
         "gmf_wfa_results": ctypes.sizeof(n.GmfWfaResults),
         "gmf_wfa_results.cigar_capacity": n.GmfWfaResults.cigar_capacity.offset,
         "gmf_wfa_results.error_flags": n.GmfWfaResults.error_flags.offset,
+        "gmf_sam_records": ctypes.sizeof(n.GmfSamRecords),
+        "gmf_sam_records.n_contigs": n.GmfSamRecords.n_contigs.offset,
+        "gmf_sam_records.tag_off": n.GmfSamRecords.tag_off.offset,
         "gmf_host_pairs": ctypes.sizeof(n.GmfHostPairs),
         "gmf_host_pairs.n_xdrop_groups": n.GmfHostPairs.n_xdrop_groups.offset,
         "gmf_host_sw_results": ctypes.sizeof(n.GmfHostSwResults),
@@ -184,3 +188,8 @@ def test_entry_points_reject_malformed_arguments_before_any_cuda_call():
     assert lib.gmf_batch_submit(None, None, None, None, None) == _native.GMF_ERR_INVALID_ARGUMENT
     assert lib.gmf_batch_poll(None, 1) == _native.GMF_ERR_INVALID_ARGUMENT
     assert lib.gmf_batch_wait(None, 1) == _native.GMF_ERR_INVALID_ARGUMENT
+    # SAM records: malformed batches refused on the host
+    assert lib.gmf_sam_count(None, None, None) == _native.GMF_ERR_INVALID_ARGUMENT
+    bad = _native.GmfSamRecords(3)  # no arrays
+    assert lib.gmf_sam_count(ctypes.byref(bad), None, None) == _native.GMF_ERR_INVALID_ARGUMENT
+    assert lib.gmf_sam_fill(ctypes.byref(bad), None, None, None) == _native.GMF_ERR_INVALID_ARGUMENT
