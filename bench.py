@@ -61,6 +61,7 @@ def parse():
     p.add_argument("--long-reads", type=int, default=200,
                    help="reads of the long-read stress leg (2,000 = the full configuration; 0 skips it)")
     p.add_argument("--wfa-pairs", type=int, default=20_000, help="pairs of the WFA leg (0: skip it)")
+    p.add_argument("--sam-records", type=int, default=25_000, help="records of the SAM leg (0: skip it)")
     p.add_argument("--serve-loads", default="10000,20000", help="offered loads of the serving leg, reads/s")
     p.add_argument("--serve-requests", type=int, default=600)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -437,6 +438,11 @@ def run_b200(args):
     if args.wfa_pairs > 0:
         wfa_res = wfa_leg(args, device, stream, flush, seed=8 + 1000 * rank, warm=warm)
 
+    # ---- SAM text of alignment records ----
+    sam_res = None
+    if args.sam_records > 0:
+        sam_res = sam_leg(args, device, stream, flush, warm=warm)
+
     # ---- serving loop: Poisson requests of 1-64 mixed-profile reads ----
     serve = None
     if not args.no_serve:
@@ -523,6 +529,11 @@ def run_b200(args):
         line["long_reads"] = longr
     if wfa_res:
         line["wfa"] = wfa_res
+    if sam_res:
+        sam_res["roofline"]["peak"] = peaks["hbm_gbs"]
+        sam_res["roofline"]["frac"] = sam_res["roofline"]["achieved"] / peaks["hbm_gbs"]
+        sam_res["roofline"]["peak_source"] = peak_src
+        line["sam"] = sam_res
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ps, head["params"])
     return line
@@ -601,6 +612,127 @@ def wfa_leg(args, device, stream, flush, seed: int, warm: int) -> dict:
                                "cores": 1, "kind": "port",
                                "sample": f"{done} random pairs of the workload, oracle_wfa_align, one thread"}
     return out
+
+
+def sam_records_workload(n: int, seed: int):
+    """Alignment records of mixed-length reads (150 bp - 20 kb, both
+    strands, soft clips, every 31st unmapped) with their reads."""
+    from types import SimpleNamespace
+
+    from graphmambaformer_b200.records import AlignmentRecord, ReadAlignments
+
+    rng = np.random.default_rng(seed)
+    lens = np.clip(rng.lognormal(7.0, 1.2, size=n), 150, 20_000).astype(np.int64)
+    pool = rng.choice(np.frombuffer(b"ACGT", np.uint8), size=int(lens.sum()))
+    results, reads, o = [], [], 0
+    for i, L in enumerate(lens):
+        L = int(L)
+        seq = pool[o: o + L].tobytes().decode()
+        o += L
+        cl, cr = int(rng.integers(0, 40)), int(rng.integers(0, 40))
+        mid = L - cl - cr
+        cigar = [("S", cl), ("=", mid // 3), ("X", 1), ("=", mid // 3), ("I", 2), ("=", mid - 2 * (mid // 3) - 3),
+                 ("D", 3), ("S", cr)]
+        cigar = [x for x in cigar if x[1] > 0]
+        rs = int(rng.integers(0, 10 ** 8))
+        rec = AlignmentRecord(read_id=f"read{i}", read_len=L, ref_id=0, ref_start=rs, ref_end=rs + mid,
+                              strand=1 if i % 2 else -1, mapq=int(rng.integers(0, 61)), cigar=cigar,
+                              is_mapped=i % 31 != 0)
+        results.append(ReadAlignments(read_id=rec.read_id, read_len=L, records=[rec]))
+        reads.append(SimpleNamespace(read_id=rec.read_id, seq=seq,
+                                     quals=rng.integers(0, 60, size=L).tolist() if i % 4 == 0 else None,
+                                     modality="ont"))
+    return results, reads
+
+
+def sam_leg(args, device, stream, flush, warm: int) -> dict:
+    """SAM text of alignment records (graphmambaformer_b200.records): device
+    time of gmf_sam_count + scan + gmf_sam_fill on device-resident records;
+    end to end from the host layout (render_sam: copies in, kernels, text
+    out); the host layout itself (sam_records) timed apart; the oracle's
+    Python rendering on a sample."""
+    import ctypes
+
+    import torch
+
+    from graphmambaformer_b200 import _native
+    from graphmambaformer_b200.device import to_device
+    from graphmambaformer_b200.records import render_sam, sam_records
+
+    results, reads = sam_records_workload(args.sam_records, seed=9)
+    t0 = time.perf_counter()
+    b = sam_records(results, reads, "ont", False, {0: 10 ** 9})
+    layout_ms = (time.perf_counter() - t0) * 1e3
+    n = len(b)
+    d = {k: to_device(getattr(b, k), device) for k in ("names", "name_off", "seq", "seq_off", "qual", "contig",
+                                                        "contig_names", "contig_off", "ref_start", "ref_end",
+                                                        "strand", "mapq", "cigar", "cigar_start", "cigar_len",
+                                                        "tags", "tag_off")}
+    p = {k: v.data_ptr() for k, v in d.items()}
+    rec = _native.GmfSamRecords(n, p["names"], p["name_off"], p["seq"], p["seq_off"], p["qual"], p["contig"],
+                                p["contig_names"], p["contig_off"], len(b.contig_off) - 1, p["ref_start"],
+                                p["ref_end"], p["strand"], p["mapq"], p["cigar"], p["cigar_start"], p["cigar_len"],
+                                None, None, p["tags"], p["tag_off"])
+    lens = torch.empty(n, dtype=torch.int64, device=device)
+    off = torch.zeros(n + 1, dtype=torch.int64, device=device)
+    sp = int(stream.cuda_stream)
+    lib = _native.lib()
+    _native.check("gmf_sam_count", lib.gmf_sam_count(ctypes.byref(rec), ctypes.c_void_p(lens.data_ptr()),
+                                                     ctypes.c_void_p(sp)))
+    torch.cumsum(lens, 0, out=off[1:])
+    total = int(off[-1].item())
+    text = torch.empty(total, dtype=torch.uint8, device=device)
+
+    def step():
+        lib.gmf_sam_count(ctypes.byref(rec), ctypes.c_void_p(lens.data_ptr()), ctypes.c_void_p(sp))
+        torch.cumsum(lens, 0, out=off[1:])
+        lib.gmf_sam_fill(ctypes.byref(rec), ctypes.c_void_p(off.data_ptr()), ctypes.c_void_p(text.data_ptr()),
+                         ctypes.c_void_p(sp))
+
+    for _ in range(warm):
+        step()
+    torch.cuda.synchronize(device)
+    ms = float(np.mean(time_device(step, args.steps, stream, flush)))
+    # algorithmic bytes of one step: both passes read each record's 69 B of fields and its CIGAR words; the
+    # fill pass reads names, bases, qualities and tags once and writes the text; the count pass writes 8 B
+    read_b = int(2 * (69 * n + 4 * b.cigar.size) + b.names.size + b.seq.size + b.qual.size + b.tags.size)
+    alg = read_b + total + 8 * n
+    h2d = int(sum(getattr(b, k).nbytes for k in ("names", "name_off", "seq", "seq_off", "qual", "contig",
+                                                  "contig_names", "contig_off", "ref_start", "ref_end", "strand",
+                                                  "mapq", "cigar", "cigar_start", "cigar_len", "tags", "tag_off")))
+    e = []
+    for _ in range(max(2, args.steps // 4)):
+        t0 = time.perf_counter()
+        out = render_sam(b, device)
+        e.append((time.perf_counter() - t0) * 1e3)
+    e_ms = float(np.mean(e))
+    res = {
+        "value": n / (ms * 1e-3), "unit": "records/s", "ms_per_step": ms,
+        "text_gb_per_s": total / (ms * 1e-3) / 1e9,
+        "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "unit": "GB/s",
+                     "bytes_per_step": alg, "text_bytes": total},
+        "e2e": {"value": n / (e_ms * 1e-3), "unit": "records/s", "ms_per_step": e_ms,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": len(out),
+                "timing": "render_sam: host arrays in, SAM bytes out"},
+        "host_layout_ms": layout_ms,
+        "config": {"workload": "sam_records_mixed", "records": n, "bases": int(b.seq.size),
+                   "read_len": "lognormal(7.0, 1.2) clipped to 150-20000", "strands": "alternating",
+                   "qualities": "every 4th read", "unmapped": "every 31st"},
+        "gpu_launches_per_step": 3,
+    }
+    if not args.no_cpu_baseline:
+        from oracle import sam
+
+        t0 = time.perf_counter()
+        k = 0
+        while k < n and time.perf_counter() - t0 < 10.0:
+            r, rd = results[k].records[0], reads[k]
+            sam.render(sam.segment(vars(r), rd.seq, rd.quals, "ont", {0: 0}), ["ref0"])
+            k += 1
+        dt = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": k / dt, "unit": "records/s", "cores": 1, "kind": "port",
+                               "sample": f"first {k} records, oracle segment + render (Python), one thread"}
+    return res
 
 
 def long_read_leg(args, device, stream, flush, seed: int, warm: int) -> dict:

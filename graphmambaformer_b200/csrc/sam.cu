@@ -237,15 +237,33 @@ __global__ void __launch_bounds__(SAM_WARPS * 32) sam_kernel(gmf_sam_records R, 
             p[6] = '\t';
         }
         p += 7;
-        // SEQ and QUAL
+        // SEQ and QUAL: each lane loads 8 bases (and qualities) before it
+        // stores any, so a long record keeps 8 loads per lane in flight
         const long long L = x.seq_len;
-        for (long long i = lane; i < L; i += 32) {
-            const long long src = x.rev ? L - 1 - i : i;
-            const char b = R.seq[x.seq0 + src];
-            p[i] = x.rev ? comp_base(b) : b;
-            int qv = R.qual ? (int)R.qual[x.seq0 + src] : 0;
-            qv = qv < 0 ? 0 : (qv > 93 ? 93 : qv);
-            p[L + 1 + i] = (char)(33 + qv);
+        constexpr int U = 8;
+        for (long long i0 = 0; i0 < L; i0 += 32 * U) {
+            char b[U];
+            int qv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const long long i = i0 + u * 32 + lane;
+                b[u] = 'N';
+                qv[u] = 0;
+                if (i < L) {
+                    const long long src = x.seq0 + (x.rev ? L - 1 - i : i);
+                    b[u] = __ldg(R.seq + src);
+                    qv[u] = R.qual ? (int)__ldg(R.qual + src) : 0;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const long long i = i0 + u * 32 + lane;
+                if (i < L) {
+                    p[i] = x.rev ? comp_base(b[u]) : b[u];
+                    const int q = qv[u] > 93 ? 93 : qv[u];
+                    p[L + 1 + i] = (char)(33 + q);
+                }
+            }
         }
         if (lane == 0) p[L] = '\t';
         p += 2 * L + 1;
