@@ -258,10 +258,13 @@ def sam_records(results: Sequence[ReadAlignments], reads: Sequence, modality: st
         if not include_secondary:
             prim = next((r for r in recs if r.is_primary), None)
             recs = [prim] if prim is not None else recs[:1]
-        qv = list(q) if q else [0] * len(seq)
-        if len(qv) < len(seq):
-            qv = qv + [0] * (len(seq) - len(qv))
-        qb = np.clip(np.asarray(qv[: len(seq)], np.int64), 0, MAX_PHRED).astype(np.uint8).tobytes()
+        if q is not None and len(q):  # padded with 0 / cut to the bases, clamped to [0, 93]
+            qa = np.zeros(len(seq), np.int64)
+            qv = np.asarray(q, np.int64)[: len(seq)]
+            qa[: len(qv)] = qv
+            qb = np.clip(qa, 0, MAX_PHRED).astype(np.uint8).tobytes()
+        else:
+            qb = bytes(len(seq))
         sb = seq.encode("ascii", errors="replace")
         for rec in recs:
             if rec is None:
