@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <unordered_set>
 #include <vector>
 
@@ -104,6 +105,27 @@ int finalize(Slot& s) {
     }
     s.ticket = -1;
     return GMF_OK;
+}
+
+// memcpy split over host threads for large copies (one thread copies a few
+// GB/s; the staging of a large batch is hundreds of MB).
+void par_memcpy(char* dst, const char* src, size_t n) {
+    constexpr size_t PIECE = 16u << 20;
+    const unsigned hw = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    const size_t parts = std::min<size_t>(hw, (n + PIECE - 1) / PIECE);
+    if (parts <= 1) {
+        if (n) std::memcpy(dst, src, n);
+        return;
+    }
+    const size_t step = (n + parts - 1) / parts;
+    std::vector<std::thread> ts;
+    ts.reserve(parts - 1);
+    for (size_t i = 1; i < parts; ++i) {
+        const size_t a = i * step, b = std::min(n, a + step);
+        if (a < b) ts.emplace_back([=] { std::memcpy(dst + a, src + a, b - a); });
+    }
+    std::memcpy(dst, src, std::min(n, step));
+    for (auto& t : ts) t.join();
 }
 
 int check_host(const gmf_host_pairs* p, const gmf_sw_params* prm, const gmf_host_sw_results* r) {
@@ -272,9 +294,9 @@ extern "C" int gmf_batch_submit(gmf_ctx* c, const gmf_host_pairs* p, const gmf_s
     }
     // stage the inputs and copy them over in one piece
     char* h = s.host;
-    if (nq) std::memcpy(h + L.q, p->query, (size_t)nq);
+    if (nq) par_memcpy(h + L.q, reinterpret_cast<const char*>(p->query), (size_t)nq);
     std::memcpy(h + L.qo, p->query_off, 8 * ((size_t)n + 1));
-    if (nt) std::memcpy(h + L.t, p->target, (size_t)nt);
+    if (nt) par_memcpy(h + L.t, reinterpret_cast<const char*>(p->target), (size_t)nt);
     std::memcpy(h + L.to, p->target_off, 8 * ((size_t)n + 1));
     std::memcpy(h + L.hb, p->half_band, 4 * (size_t)n);
     std::memcpy(h + L.off, p->band_offset, 4 * (size_t)n);

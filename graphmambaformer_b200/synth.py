@@ -498,24 +498,35 @@ def poisson_requests(n_requests: int, reads_per_s: float, pool_size: int, seed: 
 
 
 def long_reads_ont(n_reads: int = 2000, seed: int = 6, ref_len: int = 50_000_000, min_len: int = 50_000,
-                   max_len: int = 100_000, k: int = 15, w: int = 10, profile: ErrorProfile = ONT) -> ReadPool:
+                   max_len: int = 100_000, k: int = 15, w: int = 10, profile: ErrorProfile = ONT,
+                   seeder=None) -> ReadPool:
     """Long-read stress workload: ONT-like reads (5% error, 60% indels) of
     uniform length in [min_len, max_len], random strand and position on a
     seeded reference, with raw (k, w) minimizer anchors in both
-    orientations (about 10k per read)."""
+    orientations (about 10k per read).  ``seeder(ref)``, when given, returns
+    an object whose ``seed(reads)`` gives the anchors (the device minimizer
+    index); otherwise the host sketch finds them."""
     rng = np.random.default_rng(seed)
     ref = random_reference(ref_len, rng)
-    sketch = MinimizerSketch(ref, k=k, w=w)
     lens = rng.integers(min_len, max_len + 1, size=n_reads)
     strands = np.where(rng.random(n_reads) < 0.5, 1, -1)
     starts = rng.integers(0, ref_len - max_len - 1, size=n_reads)
-    reads, rp, fp, ln, st, counts = [], [], [], [], [], []
+    reads = []
     for r in range(n_reads):
         tmpl = ref[starts[r]: starts[r] + lens[r]]
         if strands[r] < 0:
             tmpl = reverse_complement(tmpl)
-        read = apply_errors(tmpl, profile, rng)
-        reads.append(read)
+        reads.append(apply_errors(tmpl, profile, rng))
+    meta = dict(workload="long_reads_ont", seed=seed, ref_len=ref_len)
+    if seeder is not None:
+        a = seeder(ref).seed(reads)
+        batch = AnchorBatch(a.read_off.astype(np.int64), a.read_pos.astype(np.int32), a.ref_pos.astype(np.int32),
+                            a.length.astype(np.int32), a.strand.astype(np.int8),
+                            np.array([len(x) for x in reads], np.int64), dict(meta, seeding="device index"))
+        return ReadPool(ref, reads, batch, np.full(n_reads, 2, np.int8))
+    sketch = MinimizerSketch(ref, k=k, w=w)
+    rp, fp, ln, st, counts = [], [], [], [], []
+    for read in reads:
         n = 0
         for s, codes in ((1, read), (-1, reverse_complement(read))):
             a, b = sketch.query(codes)
@@ -529,6 +540,5 @@ def long_reads_ont(n_reads: int = 2000, seed: int = 6, ref_len: int = 50_000_000
     np.cumsum(counts, out=off[1:])
     batch = AnchorBatch(off, np.concatenate(rp).astype(np.int32), np.concatenate(fp).astype(np.int32),
                         np.concatenate(ln).astype(np.int32), np.concatenate(st).astype(np.int8),
-                        np.array([len(x) for x in reads], np.int64),
-                        dict(workload="long_reads_ont", seed=seed, ref_len=ref_len))
+                        np.array([len(x) for x in reads], np.int64), meta)
     return ReadPool(ref, reads, batch, np.full(n_reads, 2, np.int8))
