@@ -35,7 +35,6 @@ namespace {
 
 constexpr int WFA_WARPS = 8;                          // warps per block
 constexpr int WFA_SMEM_S = 255;                       // wavefronts up to this score in shared memory
-constexpr int WFA_SMEM_CEN = WFA_SMEM_S + 1;          // index of diagonal 0 in a shared wavefront
 constexpr int WFA_SMEM_WF = 2 * WFA_SMEM_S + 3;       // ints per shared wavefront
 constexpr int WFA_MAX_BLOCKS_PER_SM = 4;
 constexpr int WFA_BLOCK_S = (WFA_WARPS * WFA_SMEM_WF - 3) / 2;  // block-wide wavefronts: scores up to 2050
@@ -49,12 +48,6 @@ struct Seq {
     __device__ unsigned ld(long long i) const {
         i = i < 0 ? 0 : (i >= nw ? nw - 1 : i);
         return __ldg(w + i);
-    }
-    // 4 codes starting at code `x` of the pair that begins at code `p0` of the buffer
-    __device__ unsigned get4(long long p0, int x) const {
-        const long long b = base + p0 + x;
-        const long long wi = b >> 2;
-        return __funnelshift_r(ld(wi), ld(wi + 1), (int)(b & 3) * 8);
     }
 };
 
