@@ -696,7 +696,7 @@ def sam_leg(args, device, stream, flush, warm: int) -> dict:
     rec = _native.GmfSamRecords(n, p["names"], p["name_off"], p["seq"], p["seq_off"], p["qual"], p["contig"],
                                 p["contig_names"], p["contig_off"], len(b.contig_off) - 1, p["ref_start"],
                                 p["ref_end"], p["strand"], p["mapq"], p["cigar"], p["cigar_start"], p["cigar_len"],
-                                None, None, p["tags"], p["tag_off"])
+                                None, None, p["tags"], p["tag_off"], int(np.diff(b.seq_off).max()))
     lens = torch.empty(n, dtype=torch.int64, device=device)
     off = torch.zeros(n + 1, dtype=torch.int64, device=device)
     sp = int(stream.cuda_stream)

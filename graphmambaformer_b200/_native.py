@@ -222,6 +222,7 @@ class GmfSamRecords(Structure):
         ("clip_right", c_void_p),
         ("tags", c_void_p),
         ("tag_off", c_void_p),
+        ("max_seq_len", c_int64),
     ]
 
 

@@ -16,7 +16,10 @@
 // caller scans them to offsets; the fill pass writes each line at its
 // offset.  Lanes copy the name, bases, qualities and tags in parallel; the
 // CIGAR runs are rendered 32 at a time with a warp scan of their text
-// lengths.
+// lengths.  The fill grid's second dimension splits the bases and qualities
+// of long records into chunks of 2,048, each copied by a warp of its own
+// (chunk 0 by the warp that writes the rest of the line), so a 20 kb read
+// does not hold one warp for the whole pass.
 
 #include "gmf_common.cuh"
 
@@ -161,12 +164,70 @@ __device__ long long line_length(const gmf_sam_records& R, const Rec& x) {
     return n + 1;  // newline
 }
 
+// Bases [lo, hi) of a record's SEQ and QUAL columns (SEQ at p, QUAL at
+// p + L + 1): each lane loads 8 bases (and qualities) before it stores any,
+// so a long stretch keeps 8 loads per lane in flight.
+__device__ __forceinline__ void copy_bases(const gmf_sam_records& R, long long seq0, long long L, bool rev, char* p,
+                                           long long lo, long long hi, int lane) {
+    constexpr int U = 8;
+    for (long long i0 = lo; i0 < hi; i0 += 32 * U) {
+        char b[U];
+        int qv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const long long i = i0 + u * 32 + lane;
+            b[u] = 'N';
+            qv[u] = 0;
+            if (i < hi) {
+                const long long src = seq0 + (rev ? L - 1 - i : i);
+                b[u] = __ldg(R.seq + src);
+                qv[u] = R.qual ? (int)__ldg(R.qual + src) : 0;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const long long i = i0 + u * 32 + lane;
+            if (i < hi) {
+                p[i] = rev ? comp_base(b[u]) : b[u];
+                const int q = qv[u] > 93 ? 93 : qv[u];
+                p[L + 1 + i] = (char)(33 + q);
+            }
+        }
+    }
+}
+
+// Bases of chunk `y` of a record: [y*ch, (y+1)*ch), the last chunk of the
+// grid taking everything to the end (so a low length hint stays correct).
+__device__ __forceinline__ void chunk_range(long long L, long long ch, int y, int ny, long long& lo, long long& hi) {
+    lo = (long long)y * ch;
+    hi = (y == ny - 1) ? L : (lo + ch < L ? lo + ch : L);
+    if (lo > L) lo = L;
+}
+
 template <bool FILL>
 __global__ void __launch_bounds__(SAM_WARPS * 32) sam_kernel(gmf_sam_records R, int64_t* line_len,
-                                                           const int64_t* line_off, char* out) {
+                                                           const int64_t* line_off, char* out, long long ch) {
     const int lane = threadIdx.x & 31;
     const int gw = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
     const int nw = (int)((gridDim.x * (unsigned)blockDim.x) >> 5);
+    const int y = FILL ? (int)blockIdx.y : 0, ny = FILL ? (int)gridDim.y : 1;
+    if (FILL && y > 0) {  // a later chunk of the bases: placed from the end of the line
+        for (int r = gw; r < R.n_records; r += nw) {
+            const long long s0 = R.seq_off[r], L = R.seq_off[r + 1] - s0;
+            long long lo, hi;
+            chunk_range(L, ch, y, ny, lo, hi);
+            if (lo >= hi) continue;
+            const long long tag_len = R.tag_off ? R.tag_off[r + 1] - R.tag_off[r] : 0;
+            const int c = R.contig[r];
+            const bool words = R.cigar_len[r] > 0 || (R.clip_left && R.clip_left[r] > 0) ||
+                               (R.clip_right && R.clip_right[r] > 0);
+            const bool rev = c >= 0 && c < R.n_contigs && L > 0 && R.ref_end[r] > R.ref_start[r] && words &&
+                             R.strand[r] == -1;  // reoriented before the length check, as the first chunk is
+            char* p = out + line_off[r + 1] - 1 - (tag_len > 0 ? 1 + tag_len : 0) - (2 * L + 1);
+            copy_bases(R, s0, L, rev, p, lo, hi, lane);
+        }
+        return;
+    }
     for (int r = gw; r < R.n_records; r += nw) {
         const Rec x = load_rec(R, r, lane);
         if (!FILL) {
@@ -237,33 +298,12 @@ __global__ void __launch_bounds__(SAM_WARPS * 32) sam_kernel(gmf_sam_records R, 
             p[6] = '\t';
         }
         p += 7;
-        // SEQ and QUAL: each lane loads 8 bases (and qualities) before it
-        // stores any, so a long record keeps 8 loads per lane in flight
+        // SEQ and QUAL: this warp copies chunk 0 of the bases
         const long long L = x.seq_len;
-        constexpr int U = 8;
-        for (long long i0 = 0; i0 < L; i0 += 32 * U) {
-            char b[U];
-            int qv[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const long long i = i0 + u * 32 + lane;
-                b[u] = 'N';
-                qv[u] = 0;
-                if (i < L) {
-                    const long long src = x.seq0 + (x.rev ? L - 1 - i : i);
-                    b[u] = __ldg(R.seq + src);
-                    qv[u] = R.qual ? (int)__ldg(R.qual + src) : 0;
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const long long i = i0 + u * 32 + lane;
-                if (i < L) {
-                    p[i] = x.rev ? comp_base(b[u]) : b[u];
-                    const int q = qv[u] > 93 ? 93 : qv[u];
-                    p[L + 1 + i] = (char)(33 + q);
-                }
-            }
+        {
+            long long lo, hi;
+            chunk_range(L, ch, 0, ny, lo, hi);
+            copy_bases(R, x.seq0, L, x.rev, p, lo, hi, lane);
         }
         if (lane == 0) p[L] = '\t';
         p += 2 * L + 1;
@@ -292,6 +332,8 @@ int grid_of(int n) {
     return (int)(blocks < 148 * 16 ? (blocks > 0 ? blocks : 1) : 148 * 16);
 }
 
+constexpr long long SAM_CHUNK = 2048;  // bases per warp in the fill pass
+
 }  // namespace
 
 extern "C" int gmf_sam_count(const gmf_sam_records* records, int64_t* line_len, gmf_stream_t stream) {
@@ -299,8 +341,8 @@ extern "C" int gmf_sam_count(const gmf_sam_records* records, int64_t* line_len, 
     if (records->n_records == 0) return GMF_OK;
     if (!line_len) return GMF_ERR_INVALID_ARGUMENT;
     GMF_TRY(gmf::bind_stream_device((cudaStream_t)stream));
-    sam_kernel<false><<<grid_of(records->n_records), SAM_WARPS * 32, 0, (cudaStream_t)stream>>>(*records, line_len,
-                                                                                             nullptr, nullptr);
+    sam_kernel<false><<<grid_of(records->n_records), SAM_WARPS * 32, 0, (cudaStream_t)stream>>>(
+        *records, line_len, nullptr, nullptr, SAM_CHUNK);
     return gmf::cuda_status(cudaGetLastError());
 }
 
@@ -310,7 +352,13 @@ extern "C" int gmf_sam_fill(const gmf_sam_records* records, const int64_t* line_
     if (records->n_records == 0) return GMF_OK;
     if (!line_off || !text) return GMF_ERR_INVALID_ARGUMENT;
     GMF_TRY(gmf::bind_stream_device((cudaStream_t)stream));
-    sam_kernel<true><<<grid_of(records->n_records), SAM_WARPS * 32, 0, (cudaStream_t)stream>>>(*records, nullptr,
-                                                                                            line_off, text);
+    // chunks of the longest record's bases (the last chunk takes any remainder)
+    const long long mx = records->max_seq_len > 0 ? records->max_seq_len : 0;
+    long long ny = (mx + SAM_CHUNK - 1) / SAM_CHUNK;
+    ny = ny < 1 ? 1 : (ny > 65535 ? 65535 : ny);
+    const long long ch = ny > 1 ? (mx + ny - 1) / ny : SAM_CHUNK;
+    const dim3 grid((unsigned)grid_of(records->n_records), (unsigned)ny);
+    sam_kernel<true><<<grid, SAM_WARPS * 32, 0, (cudaStream_t)stream>>>(*records, nullptr, line_off, text,
+                                                                     ch < SAM_CHUNK ? SAM_CHUNK : ch);
     return gmf::cuda_status(cudaGetLastError());
 }

@@ -320,9 +320,11 @@ def sam_header(references: Optional[dict], contig_names: Optional[dict], modalit
     return "\n".join(lines) + "\n"
 
 
-def render_sam(batch: SamBatch, device=None, stream: Optional[torch.cuda.Stream] = None) -> bytes:
+def render_sam(batch: SamBatch, device=None, stream: Optional[torch.cuda.Stream] = None,
+               max_seq_len: Optional[int] = None) -> bytes:
     """The records' SAM lines, rendered on the device (two launches and one
-    scan), as bytes."""
+    scan), as bytes.  ``max_seq_len`` overrides the longest-record hint that
+    splits the fill pass (it changes speed only)."""
     dev = require_cuda(device)
     n = len(batch)
     if n == 0:
@@ -338,7 +340,7 @@ def render_sam(batch: SamBatch, device=None, stream: Optional[torch.cuda.Stream]
     rec = _native.GmfSamRecords(n, p["name"], p["name_off"], p["seq"], p["seq_off"], p["qual"], p["contig"],
                                 p["contig_names"], p["contig_off"], len(batch.contig_off) - 1, p["ref_start"],
                                 p["ref_end"], p["strand"], p["mapq"], p["cigar"], p["cigar_start"], p["cigar_len"],
-                                None, None, p["tags"], p["tag_off"])
+                                None, None, p["tags"], p["tag_off"], int(np.diff(batch.seq_off).max()) if max_seq_len is None else int(max_seq_len))
     sp = stream_handle(stream, dev)
     bind(dev, sp)
     lens = torch.empty(n, dtype=torch.int64, device=dev)

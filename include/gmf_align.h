@@ -440,13 +440,15 @@ typedef struct {
     const int32_t* clip_right;   /* adjacent S word */
     const char* tags;            /* optional tag text per record (tab-separated fields), NULL = none */
     const int64_t* tag_off;      /* n_records+1 with tags */
+    int64_t max_seq_len;         /* HOST value: the longest record's bases (splits the fill pass over
+                                    more warps; 0 or too low costs speed, never correctness) */
 } gmf_sam_records;
 
 /* Length in bytes of every record's line (newline included). */
 int gmf_sam_count(const gmf_sam_records* records, int64_t* line_len, gmf_stream_t stream);
 
-/* Write every record's line at text + line_off[r] (the exclusive scan of the
- * lengths).  Replaces data/formats.py L343-397 (_make_segment) and the SAM
+/* Write every record's line at text + line_off[r], where line_off holds
+ * n_records+1 entries: the exclusive scan of the lengths and their total.  Replaces data/formats.py L343-397 (_make_segment) and the SAM
  * rendering of write_sam (L476-500) for single-end records. */
 int gmf_sam_fill(const gmf_sam_records* records, const int64_t* line_off, char* text, gmf_stream_t stream);
 

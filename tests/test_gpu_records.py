@@ -126,3 +126,6 @@ def test_device_sam_at_scale_matches_oracle():
     text = render_sam(b, "cuda:0")
     segs = [sam.segment(vars(r.records[0]), rd.seq, rd.quals, "ont", {0: 0}) for r, rd in zip(results, reads)]
     _check_lines(text, segs, ["ref0"])
+    # the length hint only splits the work: none, too low and too high give the same bytes
+    for hint in (0, 5000, 10**6):
+        assert render_sam(b, "cuda:0", max_seq_len=hint) == text, hint
