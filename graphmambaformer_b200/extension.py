@@ -381,6 +381,22 @@ class _RefCodes:
         return self._codes
 
 
+def wfa_extension_result(cigar: list, start: int, window_len: int, read_len: int,
+                         cfg: ExtensionConfig) -> ExtensionResult:
+    """A WFA-mode chain's result (extension.py L702-730): the whole read
+    against reference [start, start + window_len), op tallies from the CIGAR,
+    and the affine score recomputed from it in the reference's order of
+    operations."""
+    counts = {op: 0 for op in ("=", "X", "I", "D")}
+    for op, n in cigar:
+        counts[op] = counts.get(op, 0) + n
+    gap_cost = sum(cfg.gap_open + max(n - 1, 0) * cfg.gap_extend for op, n in cigar if op in ("I", "D"))
+    score = counts["="] * cfg.match_score - counts["X"] * cfg.mismatch_penalty - gap_cost
+    return ExtensionResult(score=float(score), cigar=cigar, read_start=0, read_end=read_len, ref_start=start,
+                           ref_end=start + window_len, n_match=counts["="], n_mismatch=counts["X"],
+                           n_insertion=counts["I"], n_deletion=counts["D"])
+
+
 class ExtensionEngine:
     """Stage 3 entry point (extension.py L469-641): chains -> alignments."""
 
@@ -497,16 +513,7 @@ class ExtensionEngine:
                 forward, chains, anchors, ref_codes = items[r]
                 fallback.append(((r, ci), (forward, [chains[ci]], anchors, ref_codes)))
                 continue
-            cigar = res.cigar(b)
-            counts = {op: 0 for op in ("=", "X", "I", "D")}
-            for op, n in cigar:
-                counts[op] = counts.get(op, 0) + n
-            gap_cost = sum(cfg.gap_open + max(n - 1, 0) * cfg.gap_extend for op, n in cigar if op in ("I", "D"))
-            score = counts["="] * cfg.match_score - counts["X"] * cfg.mismatch_penalty - gap_cost
-            results[r][ci] = ExtensionResult(
-                score=float(score), cigar=cigar, read_start=0, read_end=read_len, ref_start=start,
-                ref_end=start + len(ts[b]), n_match=counts["="], n_mismatch=counts["X"],
-                n_insertion=counts["I"], n_deletion=counts["D"])
+            results[r][ci] = wfa_extension_result(res.cigar(b), start, len(ts[b]), read_len, cfg)
         if fallback:  # banded SW, one chain per call as the reference re-enters extend_chains
             for (r, ci), ext in zip((k for k, _ in fallback), self._extend_sw([it for _, it in fallback])):
                 results[r][ci] = ext[0]

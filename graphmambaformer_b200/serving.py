@@ -138,7 +138,7 @@ class BatchAligner:
         nmem = h["nmem"][: R * mc].numpy().reshape(R, mc)
         mem = h["mem"][:A].numpy()
 
-        # ---- windows (extension.py L489-509), one pair per kept chain ----
+        # ---- one pair per kept chain, in read order ----
         cr, ck = np.nonzero(np.arange(mc)[None, :] < n_ch[:, None])  # (read, slot) of every chain
         C = len(cr)
         results: list = [[] for _ in range(R)]
@@ -157,29 +157,32 @@ class BatchAligner:
         if nz.any():
             starts = seg[:-1][nz]
             spread[nz] = np.maximum.reduceat(dg, starts) - np.minimum.reduceat(dg, starts)
-        cfg = self.ecfg
-        diag = span[cr, ck, 2].astype(np.int64) - span[cr, ck, 0].astype(np.int64)
+        rc = strand[cr, ck] < 0
+        sp4 = span[cr, ck].astype(np.int64)  # read_start, read_end, ref_start, ref_end
+        if self.ecfg.algorithm == "wfa":
+            ext = self._extend_wfa(R, rl, roff, reads_d, cr, rc, sp4, spread)
+        else:
+            ext = self._extend_sw(R, rl, roff, reads_d, cr, rc, sp4, spread, shared=True)
+        for c in range(C):
+            results[int(cr[c])].append(ext[c])
+        return results
+
+    def _gather(self, tag: str, reads_d, roff, rl, cr, rc, wstart, wlen) -> tuple:
+        """Queries (reverse-complemented for strand -1) and reference
+        windows of the pairs, gathered from the resident buffers."""
+        s, up, db = self.stream, self.buf.upload, self.buf.device_buf
+        sp = int(s.cuda_stream)
+        C = len(cr)
         rlen = rl[cr]
-        wstart = np.maximum(0, diag - cfg.flank)
-        wend = np.minimum(self.ref_len, diag + rlen + cfg.flank)
-        wend = np.where(wend - wstart > cfg.max_window, wstart + cfg.max_window, wend)
-        wlen = np.maximum(wend - wstart, 0)
-        hb_chain = np.minimum(cfg.half_band + spread, cfg.max_half_band)
-        hb_read = np.zeros(R, np.int64)
-        np.maximum.at(hb_read, cr, hb_chain)  # every chain of a read takes its widest band
-        hb = hb_read[cr].astype(np.int32)
-        boff = (diag - wstart).astype(np.int32)
         qoff = np.zeros(C + 1, np.int64)
         np.cumsum(rlen, out=qoff[1:])
         toff = np.zeros(C + 1, np.int64)
         np.cumsum(wlen, out=toff[1:])
-
-        # ---- queries and targets gathered from the resident buffers ----
-        qd = db("q", max(int(qoff[-1]), 1), torch.int8)
-        td = db("t", max(int(toff[-1]), 1), torch.int8)
-        qs_d, ql_d = up("qs", roff[cr], s), up("ql", rlen.astype(np.int32), s)
-        rc_d, qo_d = up("rc", (strand[cr, ck] < 0).astype(np.int8), s), up("qo", qoff, s)
-        ts_d, tl_d, to_d = up("ts", wstart, s), up("tl", wlen.astype(np.int32), s), up("to", toff, s)
+        qd = db(tag + "q", max(int(qoff[-1]), 1), torch.int8)
+        td = db(tag + "t", max(int(toff[-1]), 1), torch.int8)
+        qs_d, ql_d = up(tag + "qs", roff[cr], s), up(tag + "ql", rlen.astype(np.int32), s)
+        rc_d, qo_d = up(tag + "rc", rc.astype(np.int8), s), up(tag + "qo", qoff, s)
+        ts_d, tl_d, to_d = up(tag + "ts", wstart, s), up(tag + "tl", wlen.astype(np.int32), s), up(tag + "to", toff, s)
         self._call("gmf_gather_segments", ctypes.c_void_p(reads_d.data_ptr()), int(roff[-1]), C,
                    ctypes.c_void_p(qs_d.data_ptr()), ctypes.c_void_p(ql_d.data_ptr()),
                    ctypes.c_void_p(rc_d.data_ptr()), ctypes.c_void_p(qd.data_ptr()),
@@ -187,8 +190,34 @@ class BatchAligner:
         self._call("gmf_gather_segments", ctypes.c_void_p(self.ref_d.data_ptr()), self.ref_len, C,
                    ctypes.c_void_p(ts_d.data_ptr()), ctypes.c_void_p(tl_d.data_ptr()), None,
                    ctypes.c_void_p(td.data_ptr()), ctypes.c_void_p(to_d.data_ptr()), ctypes.c_void_p(sp))
+        return qd, qo_d, td, to_d, qoff, toff
 
-        # ---- banded SW + traceback (batched form) ----
+    def _extend_sw(self, R, rl, roff, reads_d, cr, rc, sp4, spread, shared: bool) -> list:
+        """Banded SW + traceback of the pairs (extension.py L489-641).  With
+        ``shared``, the chains of a read take its widest band and stop
+        together under x-drop, as one extend_chains call; without, every
+        chain is a call of its own (the WFA fallback)."""
+        s, up, db, dl = self.stream, self.buf.upload, self.buf.device_buf, self.buf.download
+        sp = int(s.cuda_stream)
+        cfg = self.ecfg
+        C = len(cr)
+        diag = sp4[:, 2] - sp4[:, 0]
+        rlen = rl[cr]
+        wstart = np.maximum(0, diag - cfg.flank)
+        wend = np.minimum(self.ref_len, diag + rlen + cfg.flank)
+        wend = np.where(wend - wstart > cfg.max_window, wstart + cfg.max_window, wend)
+        wlen = np.maximum(wend - wstart, 0)
+        hb = np.minimum(cfg.half_band + spread, cfg.max_half_band)
+        goff = None
+        if shared:
+            hb_read = np.zeros(R, np.int64)
+            np.maximum.at(hb_read, cr, hb)  # every chain of a read takes its widest band
+            hb = hb_read[cr]
+            goff = np.zeros(R + 1, np.int32)  # the chains of a read stop together under x-drop
+            np.cumsum(np.bincount(cr, minlength=R), out=goff[1:])
+        hb = hb.astype(np.int32)
+        boff = (diag - wstart).astype(np.int32)
+        qd, qo_d, td, to_d, qoff, toff = self._gather("s", reads_d, roff, rl, cr, rc, wstart, wlen)
         hb_d, bo_d = up("hb", hb, s), up("bo", boff, s)
         ord_d = up("ord", longest_first(rlen.astype(np.int32), hb), s)
         out = dict(score=db("sc", C, torch.int32), qe=db("qe", C, torch.int32), te=db("te", C, torch.int32),
@@ -201,12 +230,10 @@ class BatchAligner:
             C, rlen.astype(np.int32).ctypes.data_as(ctypes.c_void_p),
             wlen.astype(np.int32).ctypes.data_as(ctypes.c_void_p), hb.ctypes.data_as(ctypes.c_void_p), 1))
         sws = db("sws", need, torch.uint8)
-        # the chains of a read stop together under x-drop (pairs are in read order)
-        goff = np.zeros(R + 1, np.int32)
-        np.cumsum(n_ch, out=goff[1:])
-        go_d = up("go", goff, s)
+        go_d = up("go", goff, s) if goff is not None else None
         pairs_c = _native.GmfPairs(C, qd.data_ptr(), qo_d.data_ptr(), td.data_ptr(), to_d.data_ptr(), hb_d.data_ptr(),
-                                   bo_d.data_ptr(), ord_d.data_ptr(), int(hb.max()), go_d.data_ptr(), R)
+                                   bo_d.data_ptr(), ord_d.data_ptr(), int(hb.max()),
+                                   go_d.data_ptr() if go_d is not None else None, R if goff is not None else 0)
         sres = _native.GmfSwResults(out["score"].data_ptr(), out["qe"].data_ptr(), out["te"].data_ptr(),
                                     out["qs"].data_ptr(), out["ts"].data_ptr(), out["counts"].data_ptr(),
                                     cigar.data_ptr(), cap, out["cstart"].data_ptr(), out["clen"].data_ptr(),
@@ -226,13 +253,43 @@ class BatchAligner:
                        int(hh["err"][0]))
         if res.error_flags:
             raise RuntimeError(f"gmf_banded_sw reported error flags {res.error_flags}")
+        exts = []
         for c in range(C):  # ExtensionEngine._finish: window start and soft clips
             ext = _result(res, c)
             ext.ref_start += int(wstart[c])
             ext.ref_end += int(wstart[c])
             ext.cigar = merge_cigar([("S", ext.read_start)] + ext.cigar + [("S", int(rlen[c]) - ext.read_end)])
-            results[int(cr[c])].append(ext)
-        return results
+            exts.append(ext)
+        return exts
+
+    def _extend_wfa(self, R, rl, roff, reads_d, cr, rc, sp4, spread) -> list:
+        """The extension's wfa mode (extension.py L643-730) on the gathered
+        pairs: global wavefront alignment against the stretch the chain's
+        read-zero diagonal and net indel imply; chains beyond the distance
+        bound go to banded SW one chain per call, as the reference re-enters
+        extend_chains."""
+        from .extension import wfa_extension_result
+        from .wfa import DeviceWfaPairs, align_device_pairs
+
+        cfg = self.ecfg
+        rlen = rl[cr]
+        wstart = np.clip(sp4[:, 2] - sp4[:, 0], 0, max(self.ref_len - 1, 0))
+        net = (sp4[:, 3] - sp4[:, 2]) - (sp4[:, 1] - sp4[:, 0])
+        wend = np.minimum(self.ref_len, wstart + np.maximum(1, rlen + net))
+        wlen = np.maximum(wend - wstart, 0)
+        qd, qo_d, td, to_d, _, _ = self._gather("w", reads_d, roff, rl, cr, rc, wstart, wlen)
+        dp = DeviceWfaPairs(len(cr), qd, qo_d, td, to_d, rlen.astype(np.int32), wlen.astype(np.int32), self.device)
+        res = align_device_pairs(dp, cfg.wfa_max_distance, stream=self.stream,
+                                 workspace=lambda nb: self.buf.device_buf("wws", nb, torch.uint8))
+        exts = [None] * len(cr)
+        far = np.nonzero(res.distance < 0)[0]
+        for c in np.nonzero(res.distance >= 0)[0]:
+            exts[c] = wfa_extension_result(res.cigar(int(c)), int(wstart[c]), int(wlen[c]), int(rlen[c]), cfg)
+        if len(far):
+            for c, e in zip(far, self._extend_sw(R, rl, roff, reads_d, cr[far], rc[far], sp4[far], spread[far],
+                                                 shared=False)):
+                exts[c] = e
+        return exts
 
 
 @dataclass

@@ -90,8 +90,14 @@ def _check_bound(max_distance: int, max_len: int) -> int:
     return md
 
 
+def _ws(workspace, device: torch.device, nbytes: int) -> torch.Tensor:
+    """The caller's workspace (a callable: bytes -> uint8 device tensor) or
+    the shared grow-only one."""
+    return workspace(nbytes) if workspace is not None else WORKSPACE.get(device, nbytes)
+
+
 def wfa_distances(dp: DeviceWfaPairs, max_distance: int, stream: Optional[torch.cuda.Stream] = None,
-                  out: Optional[torch.Tensor] = None) -> torch.Tensor:
+                  out: Optional[torch.Tensor] = None, workspace=None) -> torch.Tensor:
     """Enqueue gmf_wfa_distance; returns the device int32 distances."""
     md = _check_bound(max_distance, dp.max_len)
     out = out if out is not None else torch.empty(max(dp.n, 1), dtype=torch.int32, device=dp.device)
@@ -100,7 +106,7 @@ def wfa_distances(dp: DeviceWfaPairs, max_distance: int, stream: Optional[torch.
     order = to_device(np.argsort(-(dp.h_qlen.astype(np.int64) + dp.h_tlen), kind="stable").astype(np.int32),
                       dp.device)
     need = int(_native.lib().gmf_wfa_workspace_bytes(dp.n, dp.max_len, md, 0))
-    ws = WORKSPACE.get(dp.device, need)
+    ws = _ws(workspace, dp.device, need)
     sp = stream_handle(stream, dp.device)
     bind(dp.device, sp)
     pairs = dp.c(order)
@@ -153,13 +159,13 @@ def _sub_batch(dp: DeviceWfaPairs, dist_d: torch.Tensor, h_dist: np.ndarray, idx
     return sub, d_sub, h_dist[idx]
 
 
-def _run_align(sub: DeviceWfaPairs, d_sub: torch.Tensor, h_d: np.ndarray, sp: int) -> dict:
+def _run_align(sub: DeviceWfaPairs, d_sub: torch.Tensor, h_d: np.ndarray, sp: int, workspace=None) -> dict:
     dev = sub.device
     n = sub.n
     entries = int(_native.lib().gmf_wfa_history_entries(n, np_ptr(sub.h_qlen), np_ptr(sub.h_tlen), np_ptr(h_d)))
     md = int(max(h_d.max(initial=0), 0))
     need = int(_native.lib().gmf_wfa_workspace_bytes(n, sub.max_len, md, entries))
-    ws = WORKSPACE.get(dev, need)
+    ws = _ws(workspace, dev, need)
     cap = int(sub.h_qlen.astype(np.int64).sum() + sub.h_tlen.astype(np.int64).sum() + n)
     i32 = dict(dtype=torch.int32, device=dev)
     out = dict(counts=torch.empty((n, 4), **i32), cigar=torch.empty(max(cap, 1), **i32),
@@ -182,13 +188,29 @@ def align_wfa_pairs(queries: Sequence[np.ndarray], targets: Sequence[np.ndarray]
                     traceback: bool = True, device=None, history_budget: int = HISTORY_BUDGET) -> WfaResult:
     """Host pairs in, host wavefront alignments out."""
     dp = upload_wfa_pairs(queries, targets, device)
+    return align_device_pairs(dp, max_distance, traceback=traceback, history_budget=history_budget)
+
+
+def align_device_pairs(dp: DeviceWfaPairs, max_distance: int = 4096, stream: Optional[torch.cuda.Stream] = None,
+                       traceback: bool = True, history_budget: int = HISTORY_BUDGET, workspace=None) -> WfaResult:
+    """Pairs already on the device in, host wavefront alignments out (on
+    ``stream``, default the current one; ``workspace``: a callable giving a
+    device uint8 tensor of at least the bytes asked, default the shared
+    grow-only workspace)."""
     if dp.n == 0:
         z = np.zeros(0, np.int32)
         return WfaResult(z, np.zeros((0, 4), np.int32), np.zeros(0, np.uint32), np.zeros(0, np.int64), z)
-    stream = torch.cuda.current_stream(dp.device)
+    stream = stream or torch.cuda.current_stream(dp.device)
     sp = int(stream.cuda_stream)
-    dist_d = wfa_distances(dp, max_distance, stream)
-    h_dist = dist_d.to("cpu").numpy().copy()
+    with torch.cuda.stream(stream):
+        return _align_device(dp, max_distance, stream, sp, traceback, history_budget, workspace)
+
+
+def _align_device(dp, max_distance, stream, sp, traceback, history_budget, workspace) -> WfaResult:
+    dist_d = wfa_distances(dp, max_distance, stream, workspace=workspace)
+    h_dist = dist_d.to("cpu", non_blocking=True)
+    stream.synchronize()
+    h_dist = h_dist.numpy().copy()
     if not traceback:
         return WfaResult(h_dist)
     counts = np.zeros((dp.n, 4), np.int32)
@@ -214,7 +236,7 @@ def align_wfa_pairs(queries: Sequence[np.ndarray], targets: Sequence[np.ndarray]
             sub, d_sub, h_d = dp, dist_d, h_dist
         else:
             sub, d_sub, h_d = _sub_batch(dp, dist_d, h_dist, idx)
-        out = _run_align(sub, d_sub, h_d, sp)
+        out = _run_align(sub, d_sub, h_d, sp, workspace)
         host = {k: v.to("cpu", non_blocking=True) for k, v in out.items() if k != "cigar"}
         stream.synchronize()
         if int(host["err"][0]) & _native.GMF_SWF_CAPACITY:
@@ -224,7 +246,11 @@ def align_wfa_pairs(queries: Sequence[np.ndarray], targets: Sequence[np.ndarray]
         if int(host["err"][0]) & _native.GMF_SWF_INTERNAL:
             raise RuntimeError("gmf_wfa_align: a distance does not belong to its pair")
         used = int(host["used"][0])
-        words = out["cigar"][:used].to("cpu").numpy().view(np.uint32).copy() if used else np.zeros(0, np.uint32)
+        words = np.zeros(0, np.uint32)
+        if used:
+            hw = out["cigar"][:used].to("cpu", non_blocking=True)
+            stream.synchronize()
+            words = hw.numpy().view(np.uint32).copy()
         counts[idx] = host["counts"].numpy()
         cstart[idx] = host["cstart"].numpy() + base
         clen[idx] = host["clen"].numpy()

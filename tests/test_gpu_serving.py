@@ -53,6 +53,42 @@ def test_batch_pipeline_matches_stage_objects(pool):
         assert all(_ext_equal(x, y) for x, y in zip(got[r], want[r])), r
 
 
+@pytest.mark.parametrize("bound", [4096, 30])
+def test_batch_pipeline_wfa_mode_matches_stage_objects(pool, bound):
+    """algorithm="wfa": the serving pipeline gathers the WFA windows on the
+    device and gives what AffineChainer + ExtensionEngine(wfa) give; with a
+    bound of 30 many chains fall back to banded SW one chain per call."""
+    import torch
+
+    from graphmambaformer_b200 import synth
+    from graphmambaformer_b200.chaining import AffineChainer, ChainingConfig
+    from graphmambaformer_b200.config import ExtensionConfig
+    from graphmambaformer_b200.extension import ExtensionEngine
+    from graphmambaformer_b200.serving import BatchAligner
+    from graphmambaformer_b200.types import AnchorSet
+
+    idx = np.arange(80)
+    reads, anchors = pool.take(idx)
+    ccfg, ecfg = ChainingConfig(), ExtensionConfig(algorithm="wfa", wfa_max_distance=bound)
+    ref_d = torch.from_numpy(pool.ref).to("cuda:0")
+    got = BatchAligner(ref_d, "cuda:0", ccfg, ecfg).align(reads, anchors)
+    sets = []
+    for r in range(len(reads)):
+        rp, fp, ln, st = anchors.read(r)
+        sets.append(AnchorSet.from_lists(rp, fp, ln, st, read_len=len(reads[r]), ref_len=len(pool.ref)))
+    chains = AffineChainer(ccfg, device="cuda:0").chain_batch(sets)
+    want = ExtensionEngine(ecfg, device="cuda:0").extend_batch(
+        [synth.decode_bases(x) for x in reads], chains, sets, synth.decode_bases(pool.ref))
+    assert sum(len(x) for x in want) > 0
+    n_clipped = 0
+    for r in range(len(reads)):
+        assert len(got[r]) == len(want[r]), r
+        assert all(_ext_equal(x, y) for x, y in zip(got[r], want[r])), r
+        n_clipped += sum(1 for y in want[r] if y.cigar and y.cigar[0][0] == "S")
+    if bound == 30:
+        assert n_clipped > 0  # some chains went through the banded-SW fallback (local, soft-clipped)
+
+
 def test_serving_same_alone_and_in_the_mix(pool):
     from graphmambaformer_b200 import synth
     from graphmambaformer_b200.serving import AlignServer, serve_stream
