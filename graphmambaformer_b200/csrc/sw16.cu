@@ -248,17 +248,17 @@ __device__ __forceinline__ void best16(unsigned& lb, int& pos0, int& pos1, const
     const unsigned cm = umax2(umax2(hk[0], hk[1]), umax2(hk[2], hk[3]));
     const unsigned nb = umax2(lb, cm);
     if (nb != lb) {
+        // per half, the steps before the first that reaches nb, counted for
+        // both halves at once: nb >= hk[u] in each half, so the plain
+        // subtractions do not borrow across halves, and flag2 is 1 while
+        // hk[u] < nb
+        const unsigned e0 = flag2(nb - hk[0]);
+        const unsigned e01 = e0 & flag2(nb - hk[1]);
+        const unsigned e012 = e01 & flag2(nb - hk[2]);
+        const unsigned u = e0 + e01 + e012;  // 0..3 in each half
         const unsigned inc = nb ^ lb;
-        if (inc & 0xFFFFu) {
-            const int t = lo16(nb);
-            const int u = lo16(hk[0]) == t ? 0 : (lo16(hk[1]) == t ? 1 : (lo16(hk[2]) == t ? 2 : 3));
-            pos0 = XD ? d + u : gstep + u;
-        }
-        if (inc >> 16) {
-            const int t = hi16(nb);
-            const int u = hi16(hk[0]) == t ? 0 : (hi16(hk[1]) == t ? 1 : (hi16(hk[2]) == t ? 2 : 3));
-            pos1 = XD ? d + u - 2 : gstep + u;
-        }
+        if (inc & 0xFFFFu) pos0 = (XD ? d : gstep) + (int)(u & 0xFFFFu);
+        if (inc >> 16) pos1 = (XD ? d - 2 : gstep) + (int)(u >> 16);
         lb = nb;
     }
 }
