@@ -281,6 +281,8 @@ def run_b200(args):
         return float(t.item())
 
     warm = max(args.warmup, 3)
+    # CPU baselines are timed on rank 0 of a one-GPU run only
+    args.no_cpu_baseline = args.no_cpu_baseline or world > 1 or rank != 0
     stream = torch.cuda.current_stream(device)
     flush = torch.empty(320 * 1024 * 1024 // 4, dtype=torch.int32, device=device)  # > 126 MB L2
 
