@@ -62,8 +62,7 @@ def parse():
                    help="reads of the long-read stress leg (2,000 = the full configuration; 0 skips it)")
     p.add_argument("--wfa-pairs", type=int, default=20_000, help="pairs of the WFA leg (0: skip it)")
     p.add_argument("--sam-records", type=int, default=25_000, help="records of the SAM leg (0: skip it)")
-    p.add_argument("--serve-loads", default="10000,15000",
-                   help="offered loads of the serving leg, reads/s (capacity is about 19k reads/s)")
+    p.add_argument("--serve-loads", default="10000,20000", help="offered loads of the serving leg, reads/s")
     p.add_argument("--serve-requests", type=int, default=600)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile-case", action="store_true",

@@ -38,7 +38,7 @@ from . import _native
 from .config import ExtensionConfig
 from .device import WORKSPACE, bind, np_ptr, ptr, require_cuda, stream_handle, to_device
 from .synth import PairSet, encode_bases, reverse_complement
-from .types import AnchorSet, Chain, ExtensionResult, merge_cigar, words_to_cigar
+from .types import AnchorSet, Chain, ExtensionResult, add_soft_clips, decode_words
 
 N_CODE = 5
 
@@ -237,7 +237,10 @@ class SWResult:
         s, n = int(self.cigar_start[b]), int(self.cigar_len[b])
         if n < 0:
             raise RuntimeError(f"pair {b}: CIGAR did not fit its output buffer")
-        return words_to_cigar(self.cigar_words[s: s + n])
+        dec = self.__dict__.get("_decoded")
+        if dec is None:  # every word of the batch decoded once
+            dec = self.__dict__["_decoded"] = decode_words(self.cigar_words)
+        return list(zip(dec[0][s: s + n], dec[1][s: s + n]))
 
 
 def fetch(out: SWOutputs, n: int) -> SWResult:
@@ -453,7 +456,7 @@ class ExtensionEngine:
             ext = _result(res, b)
             ext.ref_start += start
             ext.ref_end += start
-            ext.cigar = merge_cigar([("S", ext.read_start)] + ext.cigar + [("S", read_len - ext.read_end)])
+            ext.cigar = add_soft_clips(ext.cigar, ext.read_start, read_len - ext.read_end)
             out.append(ext)
         return out
 

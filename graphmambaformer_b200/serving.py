@@ -44,7 +44,7 @@ from .config import ExtensionConfig
 from .device import bind, require_cuda
 from .extension import SWResult, _result, longest_first, params_from_config
 from .session import _Buffers
-from .types import merge_cigar
+from .types import add_soft_clips
 
 
 def estimate_bytes(read_lens: np.ndarray, n_anchors: int, cfg: ExtensionConfig, max_chains: int) -> int:
@@ -258,7 +258,7 @@ class BatchAligner:
             ext = _result(res, c)
             ext.ref_start += int(wstart[c])
             ext.ref_end += int(wstart[c])
-            ext.cigar = merge_cigar([("S", ext.read_start)] + ext.cigar + [("S", int(rlen[c]) - ext.read_end)])
+            ext.cigar = add_soft_clips(ext.cigar, ext.read_start, int(rlen[c]) - ext.read_end)
             exts.append(ext)
         return exts
 

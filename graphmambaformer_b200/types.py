@@ -201,6 +201,30 @@ def cigar_ref_length(cigar: Sequence) -> int:
     return sum(n for op, n in cigar if op in ("=", "X", "M", "D", "N"))
 
 
+_OP_LETTERS = np.array(list(WORD_OPS) + ["?"] * (16 - len(WORD_OPS)))
+
+
+def decode_words(words: np.ndarray) -> tuple:
+    """Packed ``(run << 4) | op`` words -> (op letters, run lengths) as two
+    Python lists, decoded in one vectorized pass."""
+    w = np.asarray(words, dtype=np.uint32)
+    return _OP_LETTERS[w & 15].tolist(), (w >> 4).astype(np.int64).tolist()
+
+
 def words_to_cigar(words: np.ndarray) -> list:
     """Packed ``(run << 4) | op`` words -> ``[(op, run), ...]``."""
-    return [(WORD_OPS[int(w) & 15], int(w) >> 4) for w in np.asarray(words)]
+    ops, runs = decode_words(words)
+    return list(zip(ops, runs))
+
+
+def add_soft_clips(cigar: list, left: int, right: int) -> list:
+    """``merge_cigar([("S", left)] + cigar + [("S", right)])``.  A CIGAR of
+    merged runs that neither starts nor ends with S (what the device walk
+    writes) only gains the clips; anything else goes through merge_cigar."""
+    if cigar and cigar[0][0] != "S" and cigar[-1][0] != "S":
+        out = [("S", left)] if left > 0 else []
+        out.extend(cigar)
+        if right > 0:
+            out.append(("S", right))
+        return out
+    return merge_cigar([("S", left)] + list(cigar) + [("S", right)])
