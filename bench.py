@@ -841,7 +841,8 @@ def serve_leg(args, device, seed: int) -> dict:
     loads = [float(x) for x in str(args.serve_loads).split(",") if x]
     points = []
     try:
-        warm = synth.poisson_requests(40, loads[0], len(pool), seed=seed + 1)
+        # warm-up at the highest load, so every worker's grow-only buffers reach full size first
+        warm = synth.poisson_requests(120, max(loads), len(pool), seed=seed + 1)
         serve_stream(srv, pool, warm)
         for i, load in enumerate(loads):
             srv.completed.clear()
