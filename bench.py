@@ -837,7 +837,7 @@ def serve_leg(args, device, seed: int) -> dict:
 
     pool = synth.mixed_read_pool(n_reads=2000, seed=seed, ref_len=10_000_000)
     index = DeviceMinimizerIndex(pool.ref, k=15, w=10, max_occ=200, device=device)
-    srv = AlignServer(pool.ref, device, budget_bytes=8 << 30, workers=2, max_batch_reads=512, index=index).start()
+    srv = AlignServer(pool.ref, device, budget_bytes=8 << 30, workers=3, max_batch_reads=512, index=index).start()
     loads = [float(x) for x in str(args.serve_loads).split(",") if x]
     points = []
     try:
@@ -858,7 +858,7 @@ def serve_leg(args, device, seed: int) -> dict:
             "config": {"reference": "10 Mb uniform and its (k=15, w=10) minimizer index, resident on the device",
                        "requests": "1-64 bare reads, Poisson arrivals; seeding, chaining and extension on the GPU",
                        "reads": "pool of 2,000 mixed-profile reads (150 bp - 20 kb)",
-                       "budget": "8 GB", "workers": 2, "max_batch_reads": 512,
+                       "budget": "8 GB", "workers": 3, "max_batch_reads": 512,
                        "index_bytes": index.bytes}}
 
 

@@ -20,7 +20,7 @@ import torch
 
 from . import _native
 from .chaining import AnchorCSR
-from .device import bind, require_cuda, stream_handle, to_device
+from .device import bind, require_cuda, to_device
 
 
 class DeviceMinimizerIndex:
@@ -48,16 +48,19 @@ class DeviceMinimizerIndex:
         """Seed reads already on the device (codes CSR).  Returns device
         tensors read_off (n_reads + 1, per read: forward then reverse
         anchors), read_pos, ref_pos, length, strand and the anchor count."""
-        sp = stream_handle(stream, self.device)
+        s = stream or torch.cuda.current_stream(self.device)
+        sp = int(s.cuda_stream)
         bind(self.device, sp)
         idx = self.c()
-        counts = torch.empty(max(2 * n_reads, 1), dtype=torch.int64, device=self.device)
         vp = ctypes.c_void_p
-        _native.check("gmf_seed_count", _native.lib().gmf_seed_count(
-            ctypes.byref(idx), n_reads, vp(codes_d.data_ptr()), vp(read_off_d.data_ptr()), 1 if both_strands else 0,
-            vp(counts.data_ptr()), vp(sp)))
-        s = stream or torch.cuda.current_stream(self.device)
+        # every allocation and torch op on the caller's stream: the library's
+        # kernels run there, and a worker's stream is not ordered with the
+        # thread's default stream
         with torch.cuda.stream(s):
+            counts = torch.empty(max(2 * n_reads, 1), dtype=torch.int64, device=self.device)
+            _native.check("gmf_seed_count", _native.lib().gmf_seed_count(
+                ctypes.byref(idx), n_reads, vp(codes_d.data_ptr()), vp(read_off_d.data_ptr()),
+                1 if both_strands else 0, vp(counts.data_ptr()), vp(sp)))
             aoff = torch.zeros(2 * n_reads + 1, dtype=torch.int64, device=self.device)
             if n_reads:
                 torch.cumsum(counts[: 2 * n_reads], 0, out=aoff[1:])
@@ -66,11 +69,11 @@ class DeviceMinimizerIndex:
             out = dict(read_pos=torch.empty(max(total, 1), **i32), ref_pos=torch.empty(max(total, 1), **i32),
                        length=torch.empty(max(total, 1), **i32),
                        strand=torch.empty(max(total, 1), dtype=torch.int8, device=self.device))
-        _native.check("gmf_seed_fill", _native.lib().gmf_seed_fill(
-            ctypes.byref(idx), n_reads, vp(codes_d.data_ptr()), vp(read_off_d.data_ptr()), 1 if both_strands else 0,
-            vp(aoff.data_ptr()), vp(out["read_pos"].data_ptr()), vp(out["ref_pos"].data_ptr()),
-            vp(out["length"].data_ptr()), vp(out["strand"].data_ptr()), vp(sp)))
-        out["read_off"] = aoff[::2].contiguous()
+            _native.check("gmf_seed_fill", _native.lib().gmf_seed_fill(
+                ctypes.byref(idx), n_reads, vp(codes_d.data_ptr()), vp(read_off_d.data_ptr()),
+                1 if both_strands else 0, vp(aoff.data_ptr()), vp(out["read_pos"].data_ptr()),
+                vp(out["ref_pos"].data_ptr()), vp(out["length"].data_ptr()), vp(out["strand"].data_ptr()), vp(sp)))
+            out["read_off"] = aoff[::2].contiguous()
         out["n_anchors"] = total
         return out
 

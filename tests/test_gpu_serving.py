@@ -137,3 +137,30 @@ def test_device_seeding_server_matches_client_anchors(pool):
         assert len(x) == len(y)
         for cx, cy in zip(x, y):
             assert len(cx) == len(cy) and all(_ext_equal(p, q) for p, q in zip(cx, cy))
+
+
+def test_device_seeding_with_concurrent_workers(pool):
+    """Three workers seeding on the device at the same time, each on its own
+    stream, give every request what one request at a time gives (seeding
+    must keep all of its work on the worker's stream)."""
+    from graphmambaformer_b200 import synth
+    from graphmambaformer_b200.seeding import DeviceMinimizerIndex
+    from graphmambaformer_b200.serving import AlignServer
+
+    reqs = synth.poisson_requests(48, reads_per_s=20000, pool_size=len(pool), seed=28, max_reads=24)
+    idx = DeviceMinimizerIndex(pool.ref, k=15, w=10, max_occ=200, device="cuda:0")
+    one = AlignServer(pool.ref, "cuda:0", workers=1, max_batch_reads=24, index=idx).start()
+    many = AlignServer(pool.ref, "cuda:0", workers=3, max_batch_reads=24, index=idx).start()
+    try:
+        alone = [one.submit(pool.take(ix)[0]).result(timeout=300) for _, ix in reqs]
+        for _ in range(2):  # all at once, twice: batches of different requests overlap on the GPU
+            futs = [many.submit(pool.take(ix)[0]) for _, ix in reqs]
+            mixed = [f.result(timeout=300) for f in futs]
+            for a, b in zip(alone, mixed):
+                assert len(a) == len(b)
+                for ra, rb in zip(a, b):
+                    assert len(ra) == len(rb) and all(_ext_equal(x, y) for x, y in zip(ra, rb))
+    finally:
+        one.stop()
+        many.stop()
+    assert many.batches > 3
