@@ -21,6 +21,7 @@ GMF_ERR_CAPACITY = 4
 GMF_ERR_LIMIT = 5
 GMF_ERR_TIMEOUT = 6
 GMF_ERR_NOT_READY = 7
+GMF_ERR_HOST = 8
 
 GMF_SWF_WORKSPACE = 1
 GMF_SWF_CAPACITY = 2

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cstring>
 #include <mutex>
+#include <new>
 #include <thread>
 #include <unordered_set>
 #include <vector>
@@ -122,7 +123,12 @@ void par_memcpy(char* dst, const char* src, size_t n) {
     ts.reserve(parts - 1);
     for (size_t i = 1; i < parts; ++i) {
         const size_t a = i * step, b = std::min(n, a + step);
-        if (a < b) ts.emplace_back([=] { std::memcpy(dst + a, src + a, b - a); });
+        if (a >= b) continue;
+        try {
+            ts.emplace_back([=] { std::memcpy(dst + a, src + a, b - a); });
+        } catch (...) {  // no thread to spare: copy this piece here
+            std::memcpy(dst + a, src + a, b - a);
+        }
     }
     std::memcpy(dst, src, std::min(n, step));
     for (auto& t : ts) t.join();
@@ -178,14 +184,17 @@ void lpt_order(const gmf_host_pairs* p, int32_t* order) {
 
 }  // namespace
 
-extern "C" int gmf_ctx_create(int device, int32_t slots, size_t memory_budget, gmf_ctx** out) {
+static int ctx_destroy(gmf_ctx* c);
+
+static int ctx_create(int device, int32_t slots, size_t memory_budget, gmf_ctx** out) {
     if (!out || slots < 1 || slots > CTX_MAX_SLOTS) return GMF_ERR_INVALID_ARGUMENT;
     *out = nullptr;
     int ndev = 0;
     GMF_CUDA_TRY(cudaGetDeviceCount(&ndev));
     if (device < 0 || device >= ndev) return GMF_ERR_INVALID_ARGUMENT;
     GMF_CUDA_TRY(cudaSetDevice(device));
-    gmf_ctx* c = new gmf_ctx();
+    gmf_ctx* c = new (std::nothrow) gmf_ctx();
+    if (!c) return GMF_ERR_HOST;
     c->device = device;
     c->budget = memory_budget;
     c->n_slots = slots;
@@ -193,7 +202,7 @@ extern "C" int gmf_ctx_create(int device, int32_t slots, size_t memory_budget, g
         Slot& s = c->slots[i];
         if (cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) != cudaSuccess) {
-            gmf_ctx_destroy(c);
+            ctx_destroy(c);
             return GMF_ERR_CUDA;
         }
     }
@@ -201,7 +210,7 @@ extern "C" int gmf_ctx_create(int device, int32_t slots, size_t memory_budget, g
     return GMF_OK;
 }
 
-extern "C" int gmf_ctx_destroy(gmf_ctx* c) {
+static int ctx_destroy(gmf_ctx* c) {
     if (!c) return GMF_ERR_INVALID_ARGUMENT;
     cudaSetDevice(c->device);
     for (Slot& s : c->slots) {
@@ -215,8 +224,8 @@ extern "C" int gmf_ctx_destroy(gmf_ctx* c) {
     return GMF_OK;
 }
 
-extern "C" int gmf_batch_submit(gmf_ctx* c, const gmf_host_pairs* p, const gmf_sw_params* prm,
-                                const gmf_host_sw_results* r, int64_t* ticket) {
+static int batch_submit(gmf_ctx* c, const gmf_host_pairs* p, const gmf_sw_params* prm,
+                        const gmf_host_sw_results* r, int64_t* ticket) {
     if (!c || !ticket) return GMF_ERR_INVALID_ARGUMENT;
     GMF_TRY(check_host(p, prm, r));
     std::lock_guard<std::mutex> lock(c->mu);
@@ -370,6 +379,34 @@ static int complete(gmf_ctx* c, int64_t ticket, bool block) {
     return GMF_ERR_INVALID_ARGUMENT;  // unknown, or already completed
 }
 
-extern "C" int gmf_batch_poll(gmf_ctx* c, int64_t ticket) { return complete(c, ticket, false); }
+// No C++ exception leaves the library: a failed host allocation, thread or
+// lock becomes GMF_ERR_HOST.
+template <class F>
+static int guarded(F&& f) noexcept {
+    try {
+        return f();
+    } catch (...) {
+        return GMF_ERR_HOST;
+    }
+}
 
-extern "C" int gmf_batch_wait(gmf_ctx* c, int64_t ticket) { return complete(c, ticket, true); }
+extern "C" int gmf_ctx_create(int device, int32_t slots, size_t memory_budget, gmf_ctx** out) {
+    return guarded([&] { return ctx_create(device, slots, memory_budget, out); });
+}
+
+extern "C" int gmf_ctx_destroy(gmf_ctx* c) {
+    return guarded([&] { return ctx_destroy(c); });
+}
+
+extern "C" int gmf_batch_submit(gmf_ctx* c, const gmf_host_pairs* p, const gmf_sw_params* prm,
+                                const gmf_host_sw_results* r, int64_t* ticket) {
+    return guarded([&] { return batch_submit(c, p, prm, r, ticket); });
+}
+
+extern "C" int gmf_batch_poll(gmf_ctx* c, int64_t ticket) {
+    return guarded([&] { return complete(c, ticket, false); });
+}
+
+extern "C" int gmf_batch_wait(gmf_ctx* c, int64_t ticket) {
+    return guarded([&] { return complete(c, ticket, true); });
+}

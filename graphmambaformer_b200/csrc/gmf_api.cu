@@ -11,6 +11,7 @@ extern "C" const char* gmf_status_string(int status) {
         case GMF_ERR_LIMIT: return "input beyond a supported size limit";
         case GMF_ERR_TIMEOUT: return "bounded device wait expired";
         case GMF_ERR_NOT_READY: return "work still in flight";
+        case GMF_ERR_HOST: return "host resource failure";
         default: return "unknown status";
     }
 }

@@ -54,6 +54,7 @@ typedef struct CUstream_st* gmf_stream_t; /* a cudaStream_t; NULL = legacy defau
 #define GMF_ERR_LIMIT 5            /* input beyond a documented size limit */
 #define GMF_ERR_TIMEOUT 6          /* a bounded device-side wait expired */
 #define GMF_ERR_NOT_READY 7        /* asynchronous work still in flight */
+#define GMF_ERR_HOST 8             /* a host-side resource failed (memory, threads) */
 
 const char* gmf_status_string(int status);
 int gmf_version(void); /* major*10000 + minor*100 + patch */
