@@ -50,7 +50,7 @@ class _Buffers:
         h = self._grow(self.host, name, n, dt, True)
         d = self._grow(self.dev, name, n, dt, False)
         if n:
-            h[:n].numpy()[...] = a.reshape(-1)
+            h[:n].copy_(torch.from_numpy(a.reshape(-1)))  # torch's host copy runs on several threads
             with torch.cuda.stream(stream):
                 d[:n].copy_(h[:n], non_blocking=True)
         return d
