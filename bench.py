@@ -42,6 +42,7 @@ sys.path.insert(0, ROOT)
 METRIC = "banded-SW GCUPS & chain anchors/s, batched vs plain on 1 B200; p50/p99 ms"
 INT_OPS_PER_CELL = 11  # scalar-equivalent integer ops per DP cell (E, F, H, sub, best)
 TB_BYTES_PER_CELL = 0.5  # 4 traceback bits per cell written to the workspace
+CHAIN_OPS_PER_EVAL = 10  # f64 / int ops per chaining predecessor evaluation (gap, score, penalty, compares)
 
 
 def parse():
@@ -184,7 +185,34 @@ def measure_int_peak(device) -> dict:
             ms = e0.elapsed_time(e1)
             best = max(best, lib.gmf_probe_int_ops(kind, blocks, threads, iters) / (ms * 1e-3))
         res[name] = best / 1e12  # Tops/s
+    # float64 add / max (the chaining DP's arithmetic)
+    lib.gmf_probe_f64.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p, ctypes.c_void_p]
+    outd = torch.empty(blocks * threads, dtype=torch.float64, device=device)
+    best = 0.0
+    for _ in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        lib.gmf_probe_f64(blocks, threads, iters, ctypes.c_void_p(outd.data_ptr()), ctypes.c_void_p(s.cuda_stream))
+        e1.record(s)
+        e1.synchronize()
+        best = max(best, 4.0 * 8.0 * iters * blocks * threads / (e0.elapsed_time(e1) * 1e-3))
+    res["f64_add_max"] = best / 1e12
     return res
+
+
+def chain_pair_evaluations(batch, lookback: int) -> int:
+    """Predecessor evaluations of the chaining DP: per read and strand with
+    n anchors, sum over i < n of min(i, lookback)."""
+    r = np.repeat(np.arange(len(batch.read_off) - 1), np.diff(batch.read_off))
+    plus = np.bincount(r[batch.strand > 0], minlength=len(batch.read_off) - 1).astype(np.int64)
+    minus = np.diff(batch.read_off).astype(np.int64) - plus
+    h = int(lookback)
+    total = 0
+    for n in (plus, minus):
+        small = n <= h
+        total += int((n[small] * (n[small] - 1) // 2).sum())
+        total += int((h * (h - 1) // 2 + (n[~small] - h) * h).sum())
+    return total
 
 
 def load_peaks():
@@ -441,8 +469,10 @@ def run_b200(args):
             ce.append((time.perf_counter() - t0) * 1e3)
         barrier()
         ce_ms = max_over_ranks(float(np.mean(ce)))
+        evals = chain_pair_evaluations(cb, cfg.max_lookback)
         chain = {
             "value": anchors_total / (c_ms * 1e-3), "unit": "anchors/s", "ms_per_step": c_ms,
+            "pair_evaluations_per_step": evals,
             "config": cdesc, "gpu_launches_per_step": 3,
             "e2e": {"value": anchors_total / (ce_ms * 1e-3), "unit": "anchors/s", "ms_per_step": ce_ms,
                     "h2d_bytes_per_step": csess.h2d_bytes, "d2h_bytes_per_step": csess.d2h_bytes},
@@ -547,6 +577,11 @@ def run_b200(args):
                     "session": small["total"] / (small["session_ms"] * 1e-3) / 1e9},
             "gpu_launches_per_step": small["launches"]}
     if chain:
+        # about 10 f64/int ops per predecessor evaluation, against this GPU's f64 add/max rate
+        ach = CHAIN_OPS_PER_EVAL * chain["pair_evaluations_per_step"] / (chain["ms_per_step"] * 1e-3) / 1e12
+        chain["roofline"] = {"bound": "f64 issue", "achieved": ach, "peak": ip["f64_add_max"], "unit": "Tops/s",
+                             "frac": ach / ip["f64_add_max"], "ops_per_evaluation": CHAIN_OPS_PER_EVAL,
+                             "peak_source": "f64 add/max probe, this GPU"}
         line["chain"] = chain
     if serve:
         line["serving"] = serve

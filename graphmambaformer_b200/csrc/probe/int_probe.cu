@@ -82,7 +82,36 @@ __global__ void int_probe_kernel(int iters, int a, int b, int* out) {
     out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+// Float64 add / max chains (the chaining DP's arithmetic): 4 f64 ops per
+// step on each of 8 independent chains per thread.
+__global__ void f64_probe_kernel(int iters, double a, double b, double* out) {
+    double x[8], y[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        x[k] = threadIdx.x * 0.5 + k;
+        y[k] = blockIdx.x + 0.25 * k;
+    }
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            x[k] = fmax(x[k] + a, y[k]);
+            y[k] = fmax(y[k] - b, x[k]);
+        }
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += x[k] + y[k];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
 }  // namespace
+
+// Launch the float64 probe (4 * 8 * iters ops per thread).
+extern "C" int gmf_probe_f64(int blocks, int threads, int iters, double* out, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    f64_probe_kernel<<<blocks, threads, 0, s>>>(iters, 0.75, 0.5, out);
+    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
 
 // Launch one probe; the caller times it with events on `stream`.
 extern "C" int gmf_probe_int(int kind, int blocks, int threads, int iters, int* out, void* stream) {
