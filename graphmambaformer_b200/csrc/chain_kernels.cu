@@ -531,7 +531,7 @@ namespace {
 // 2048 (24 KB) for the per-strand peel, so 4 and 9 CTAs fit an SM; larger
 // reads / strands sort in their own workspace range instead.
 int sort_smem_elems() { return 4096; }
-int peel_smem_elems() { return 2048; }
+int peel_smem_elems() { return 4096; }
 
 size_t sort_smem_bytes(int elems) { return (size_t)elems * (sizeof(unsigned long long) + sizeof(int)); }
 
