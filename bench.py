@@ -70,6 +70,8 @@ def parse():
                    help="small single-GPU case for ncu captures (no timing JSON)")
     p.add_argument("--profile-longest", type=int, default=0,
                    help="with --profile-case: the N largest pairs (by DP area) of the workload")
+    p.add_argument("--profile-chain", type=int, default=0,
+                   help="with --profile-case: chain N reads of the HiFi chaining workload instead")
     return p.parse_args()
 
 
@@ -991,11 +993,25 @@ def run_reference(args):
 
 def profile_case(args):
     """A small single-GPU case for ncu captures: 2,000 pairs of the chosen
-    workload (or its N largest pairs), 3 launches of the batched form."""
+    workload (or its N largest pairs), 3 launches of the batched form; or N
+    reads of the HiFi chaining workload, 3 launches of the chaining batch."""
     import torch
 
     from graphmambaformer_b200 import extension
 
+    if args.profile_chain:
+        from graphmambaformer_b200 import chaining
+        from graphmambaformer_b200.config import ChainingConfig
+
+        cb, _ = chain_workload(args.profile_chain, seed=2)
+        cfg = ChainingConfig(max_lookback=50, max_gap=5000)
+        da = chaining.upload_anchors(cb, "cuda:0")
+        out = chaining.ChainOutputs.allocate(da, cfg.max_chains)
+        for _ in range(3):
+            chaining.launch_chain_batch(da, cfg, out=out)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_case": "done", "anchors_per_launch": cb.n_anchors}))
+        return
     if args.profile_longest:
         ps, params, _ = sw_workload(args.workload, args.pairs, seed=1)
         area = ps.query_len.astype(np.int64) * (2 * ps.half_band.astype(np.int64) + 1)

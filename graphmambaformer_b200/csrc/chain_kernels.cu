@@ -17,7 +17,9 @@
 // Layout: one CTA per read for sort and peel/select (shared-memory bitonic
 // sort of 64-bit keys + 32-bit tie index; reads too large for shared memory
 // sort in their own workspace range), one warp per (read, strand) segment for
-// the DP with the predecessor window in a shared-memory ring.
+// the DP: lanes own anchors and each finished score is broadcast to the
+// window (up to 224 predecessors), or, for wider windows, the window sits in
+// a shared-memory ring and a warp reduction picks each anchor's predecessor.
 
 #include <float.h>
 
@@ -286,6 +288,102 @@ __global__ void __launch_bounds__(128) chain_dp_kernel(DpArgs a) {
     }
 }
 
+// The same recurrence with the anchors owned by lanes: lane l holds anchor
+// 32(b+k) + l of K consecutive blocks of 32 (K - 1 blocks cover the window).
+// Step t finalises anchor t (its owner's running maximum against w_t),
+// broadcasts (f_t, read_end_t, ref_end_t), and every anchor i with
+// 1 <= i - t <= lb folds the candidate of predecessor t into its running
+// maximum.  Candidates arrive in ascending j and replace the maximum only when
+// strictly larger, so the first maximum (lowest j) wins as in the reference;
+// each candidate is the same float64 add / subtract.  After 32 steps the
+// finished block is stored (coalesced) and the next block is loaded.
+__device__ __forceinline__ void dp_load_slot(const DpArgs& a, int64_t st, int64_t r0, int i, int n,
+                                             int& q, int& r, double& w) {
+    if (i < n) {
+        const int64_t gi = st + i;
+        q = a.read_end[gi];
+        r = a.ref_end[gi];
+        w = a.weight ? a.weight[gi] : (double)a.length[r0 + a.perm[gi]];
+    } else {
+        q = 0;
+        r = 0;
+        w = 0.0;
+    }
+}
+
+template <int K>
+__global__ void __launch_bounds__(128) chain_dp_bcast_kernel(DpArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int wpb = blockDim.x >> 5;
+    const int lb = a.lookback > 1 ? a.lookback : 1;
+    const unsigned mg = a.max_gap > 0 ? (unsigned)a.max_gap : 0u;
+    for (int s = blockIdx.x * wpb + wib; s < a.n_segments; s += gridDim.x * wpb) {
+        int64_t st;
+        int n;
+        seg_range(a, s, st, n);
+        if (n <= 0) continue;
+        const int64_t r0 = a.row_off ? 0 : a.read_off[s >> 1];
+        int q[K], rr[K], bj[K];
+        double w[K], best[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            dp_load_slot(a, st, r0, 32 * k + lane, n, q[k], rr[k], w[k]);
+            best[k] = -DBL_MAX;
+            bj[k] = -1;
+        }
+        for (int base = 0; base < n; base += 32) {
+            const int steps = n - base < 32 ? n - base : 32;
+            bool live[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) live[k] = base + 32 * k + lane < n;
+            for (int u = 0; u < steps; ++u) {
+                const double fo = (bj[0] >= 0 && best[0] > w[0]) ? best[0] : w[0];
+                const double ft = __shfl_sync(FULL_MASK, fo, u);
+                const int qt = __shfl_sync(FULL_MASK, q[0], u);
+                const int rt = __shfl_sync(FULL_MASK, rr[0], u);
+                const int t = base + u;
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    if (32 * k - u > lb) break;  // no anchor of this block reaches back to t
+                    const int d = 32 * k + lane - u;
+                    const int dq = q[k] - qt;
+                    const int dr = rr[k] - rt;
+                    if (live[k] && (unsigned)(d - 1) < (unsigned)lb && (unsigned)(dq - 1) < mg &&
+                        (unsigned)(dr - 1) < mg) {
+                        const double mn = (double)(dq < dr ? dq : dr);
+                        const double adv = mn < w[k] ? mn : w[k];
+                        const int gap = dr > dq ? dr - dq : dq - dr;
+                        double sc = __dsub_rn(__dadd_rn(ft, adv), __ldg(&a.lut[gap]));
+                        if (a.bonus)
+                            sc = __dadd_rn(sc, __ldg(&a.bonus[(st + base + 32 * k + lane) * lb + (lb - d)]));
+                        if (bj[k] < 0 || sc > best[k]) {
+                            best[k] = sc;
+                            bj[k] = t;
+                        }
+                    }
+                }
+            }
+            if (live[0]) {
+                const bool take = bj[0] >= 0 && best[0] > w[0];
+                a.f[st + base + lane] = take ? best[0] : w[0];
+                a.parent[st + base + lane] = take ? bj[0] : -1;
+            }
+#pragma unroll
+            for (int k = 0; k + 1 < K; ++k) {
+                q[k] = q[k + 1];
+                rr[k] = rr[k + 1];
+                w[k] = w[k + 1];
+                best[k] = best[k + 1];
+                bj[k] = bj[k + 1];
+            }
+            dp_load_slot(a, st, r0, base + 32 * K + lane, n, q[K - 1], rr[K - 1], w[K - 1]);
+            best[K - 1] = -DBL_MAX;
+            bj[K - 1] = -1;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Chain peeling + select: one CTA per read.
 // ---------------------------------------------------------------------------
@@ -343,73 +441,183 @@ __global__ void __launch_bounds__(256) chain_peel_kernel(PeelArgs a) {
         if (threadIdx.x == 0) a.n_chains[r] = 0;
         return;
     }
-    // claimed flags reuse the tie-index array after the sort (one byte each)
+    __shared__ int n_start;
+    __shared__ int n_fill;
+    __shared__ int n_walk;
+    __shared__ int warp_cnt[32];
     for (int seg = 0; seg < 2; ++seg) {
         const int n = seg == 0 ? np : nm;
         const int s0 = seg == 0 ? 0 : np;  // offset of the segment inside the read
         __syncthreads();
         if (n < a.min_chain_anchors || n == 0) continue;
-        const int np2 = next_pow2(n);
+        const double* fs = a.f + a0 + s0;
+        const int32_t* par = a.parent + a0 + s0;
+        // Walk starts.  A node with a child of higher score is claimed before
+        // its own turn (the child ranks first, and the claimed set is closed
+        // under predecessors), so the walk skips it in the reference's order:
+        // only the other nodes are ranked.  dom[] marks the skipped nodes.
+        int8_t* dom = a.claimed + a0;
+        for (int x = threadIdx.x; x < n; x += blockDim.x) dom[x] = 0;
+        if (threadIdx.x == 0) {
+            n_start = 0;
+            n_fill = 0;
+        }
+        __syncthreads();
+        for (int x = threadIdx.x; x < n; x += blockDim.x) {
+            const int p = par[x];
+            if (p >= 0 && fs[x] > fs[p]) dom[p] = 1;
+        }
+        __syncthreads();
+        const int lane = threadIdx.x & 31;
+        const unsigned lt = (1u << lane) - 1u;
+        for (int x0 = threadIdx.x & ~31; x0 < n; x0 += blockDim.x) {
+            const unsigned b = __ballot_sync(FULL_MASK, x0 + lane < n && !dom[x0 + lane]);
+            if (lane == 0 && b) atomicAdd(&n_start, __popc(b));
+        }
+        __syncthreads();
+        const int ns = n_start;
+        const int np2 = next_pow2(ns);
         unsigned long long* key;
         int* idx;
         if (np2 <= a.smem_elems) {
             key = pk_smem;
             idx = reinterpret_cast<int*>(pk_smem + a.smem_elems);
         } else {
-            key = a.gkey + 2 * a0;
+            key = a.gkey + 2 * a0;  // np2 <= 2n entries of this read's range
             idx = a.gidx + 2 * a0;
         }
-        for (int x = threadIdx.x; x < np2; x += blockDim.x) {
-            if (x < n) {
+        for (int x0 = threadIdx.x & ~31; x0 < n; x0 += blockDim.x) {
+            const int x = x0 + lane;
+            const bool st = x < n && !dom[x];
+            const unsigned b = __ballot_sync(FULL_MASK, st);
+            int base = 0;
+            if (lane == 0 && b) base = atomicAdd(&n_fill, __popc(b));
+            base = __shfl_sync(FULL_MASK, base, 0);
+            if (st) {
                 // argsort(-f, stable): ascending -f == descending f, ties by index
-                key[x] = ~ordered_bits(a.f[a0 + s0 + x]);
-                idx[x] = x;
-            } else {
-                key[x] = ~0ull;
-                idx[x] = 0x7fffffff;
+                const int slot = base + __popc(b & lt);
+                key[slot] = ~ordered_bits(fs[x]);
+                idx[slot] = x;
             }
+        }
+        for (int x = ns + threadIdx.x; x < np2; x += blockDim.x) {
+            key[x] = ~0ull;
+            idx[x] = 0x7fffffff;
         }
         __syncthreads();
         block_bitonic(key, idx, np2);
         __syncthreads();
         const int c_first = n_cand;  // chains found in earlier segments
-        // the serial walk reads predecessors and claimed flags at every step:
-        // when the strand sorted in shared memory, the dead sort keys hold them
-        const bool in_smem = np2 <= a.smem_elems;
-        int8_t* claimed = in_smem ? reinterpret_cast<int8_t*>(reinterpret_cast<int32_t*>(key) + np2)
-                                  : a.claimed + a0;
-        const int32_t* par = a.parent + a0 + s0;
-        if (in_smem) {
-            int32_t* par_s = reinterpret_cast<int32_t*>(key);  // 4*np2 + np2 bytes <= 8*np2
-            for (int x = threadIdx.x; x < n; x += blockDim.x) par_s[x] = par[x];
-            par = par_s;
-        }
-        for (int x = threadIdx.x; x < n; x += blockDim.x) claimed[x] = 0;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            const double* f = a.f + a0 + s0;
-            for (int k = 0; k < n; ++k) {
-                const int i = idx[k];
-                if (claimed[i]) continue;
-                int m = 0;
-                int node = i;
-                const int moff = n_memtot;
-                while (node >= 0 && !claimed[node]) {
-                    claimed[node] = 1;
-                    a.mem_tmp[a0 + moff + m] = node;
-                    ++m;
-                    node = par[node];
+        // The walk is serial in rank order (the reference's loop): one thread
+        // takes the starts in order (the next start's index loaded ahead) and
+        // walks the unclaimed ones.  Every walk is recorded -- (member offset,
+        // count) and (start, stop node) -- and scored afterwards by the whole
+        // block.  The strand's walks claim all n nodes, so its members fill
+        // mem_tmp[mem_base, mem_base + n).
+        const int mem_base = n_memtot;
+        if (n <= a.smem_elems) {
+            // shared memory, in the dead sort keys below the sorted starts:
+            // pw[x] = predecessor + 1 with bit 31 set once claimed (one load
+            // per step of a walk), and the member list
+            int* pw = reinterpret_cast<int*>(pk_smem);
+            int* ml = pw + n;
+            for (int x = threadIdx.x; x < n; x += blockDim.x) pw[x] = par[x] + 1;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                int mo = 0, w = c_first;
+                int i_next = idx[0];
+                for (int k = 0; k < ns; ++k) {
+                    const int i = i_next;
+                    if (k + 1 < ns) i_next = idx[k + 1];
+                    int v = pw[i];
+                    if (v < 0) continue;
+                    int m = 0;
+                    int node = i;
+                    do {
+                        pw[node] = v | (int)0x80000000u;
+                        ml[mo + m] = node;
+                        ++m;
+                        node = v - 1;
+                        if (node < 0) break;
+                        v = pw[node];
+                    } while (v >= 0);
+                    a.c_mem[a0 + w] = make_int2(mem_base + mo, m);
+                    a.c_span[a0 + w] = make_int4(i, node, 0, 0);
+                    ++w;
+                    mo += m;
                 }
-                const double sc = f[i] - (node >= 0 ? f[node] : 0.0);
-                if (m < a.min_chain_anchors || sc < a.min_chain_score) continue;
-                const int c = n_cand++;
-                a.c_score[a0 + c] = sc;
-                a.c_mem[a0 + c] = make_int2(moff, m);
-                a.c_strand[a0 + c] = (int8_t)(seg == 0 ? 1 : -1);
-                n_memtot += m;
+                n_walk = w;
+            }
+            __syncthreads();
+            for (int x = threadIdx.x; x < n; x += blockDim.x) a.mem_tmp[a0 + mem_base + x] = ml[x];
+        } else {
+            int8_t* claimed = a.claimed + a0;  // held the dom flags
+            for (int x = threadIdx.x; x < n; x += blockDim.x) claimed[x] = 0;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                int mo = 0, w = c_first;
+                int i_next = idx[0];
+                for (int k = 0; k < ns; ++k) {
+                    const int i = i_next;
+                    if (k + 1 < ns) i_next = idx[k + 1];
+                    if (claimed[i]) continue;
+                    int m = 0;
+                    int node = i;
+                    while (node >= 0) {
+                        const int8_t cl = claimed[node];
+                        const int nx = par[node];
+                        if (cl) break;
+                        claimed[node] = 1;
+                        a.mem_tmp[a0 + mem_base + mo + m] = node;
+                        ++m;
+                        node = nx;
+                    }
+                    a.c_mem[a0 + w] = make_int2(mem_base + mo, m);
+                    a.c_span[a0 + w] = make_int4(i, node, 0, 0);
+                    ++w;
+                    mo += m;
+                }
+                n_walk = w;
             }
         }
         __syncthreads();
+        if (threadIdx.x == 0) n_memtot = mem_base + n;
+        // candidates: the walks with enough members and a partial score
+        // f[start] - f[stop] above the floor, kept in walk order (compacted in
+        // place, 256 records at a time: a record moves only to a lower slot)
+        {
+            const int wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+            const int n_w = n_walk;
+            for (int w0 = c_first; w0 < n_w; w0 += blockDim.x) {
+                const int w = w0 + threadIdx.x;
+                bool keep = false;
+                double sc = 0.0;
+                int2 cm = make_int2(0, 0);
+                if (w < n_w) {
+                    cm = a.c_mem[a0 + w];
+                    const int4 se = a.c_span[a0 + w];
+                    sc = fs[se.x] - (se.y >= 0 ? fs[se.y] : 0.0);
+                    keep = cm.y >= a.min_chain_anchors && sc >= a.min_chain_score;
+                }
+                const unsigned kb = __ballot_sync(FULL_MASK, keep);
+                if (lane == 0) warp_cnt[wid] = __popc(kb);
+                __syncthreads();
+                int slot = n_cand + __popc(kb & lt);
+                int tot = 0;
+                for (int q = 0; q < nwarp; ++q) {
+                    if (q < wid) slot += warp_cnt[q];
+                    tot += warp_cnt[q];
+                }
+                __syncthreads();
+                if (keep) {
+                    a.c_score[a0 + slot] = sc;
+                    a.c_mem[a0 + slot] = cm;
+                    a.c_strand[a0 + slot] = (int8_t)(seg == 0 ? 1 : -1);
+                }
+                if (threadIdx.x == 0) n_cand += tot;
+                __syncthreads();
+            }
+        }
         // spans of this segment's chains over their members' original
         // coordinates: one warp per chain, members 32 at a time
         {
@@ -562,9 +770,29 @@ int launch_sort(const gmf_anchor_batch* an, const gmf_sorted_anchors* so, unsign
     return cuda_status(cudaGetLastError());
 }
 
+template <int K>
+int launch_dp_bcast(const DpArgs& d, int n_segments, cudaStream_t stream) {
+    const int wpb = 4;
+    const int blocks = (n_segments + wpb - 1) / wpb;
+    if (blocks > 0) chain_dp_bcast_kernel<K><<<blocks, 32 * wpb, 0, stream>>>(d);
+    return cuda_status(cudaGetLastError());
+}
+
 int launch_dp(DpArgs d, int n_segments, cudaStream_t stream) {
     d.n_segments = n_segments;
     int lb = d.lookback > 1 ? d.lookback : 1;
+    // windows up to 224 predecessors: lanes own anchors, K = ceil(lb/32) + 1
+    // blocks of 32 in registers
+    switch ((lb + 31) / 32 + 1) {
+        case 2: return launch_dp_bcast<2>(d, n_segments, stream);
+        case 3: return launch_dp_bcast<3>(d, n_segments, stream);
+        case 4: return launch_dp_bcast<4>(d, n_segments, stream);
+        case 5: return launch_dp_bcast<5>(d, n_segments, stream);
+        case 6: return launch_dp_bcast<6>(d, n_segments, stream);
+        case 7: return launch_dp_bcast<7>(d, n_segments, stream);
+        case 8: return launch_dp_bcast<8>(d, n_segments, stream);
+        default: break;
+    }
     d.ring = next_pow2(lb + 1);
     const int wpb = 4;
     const size_t smem = (size_t)wpb * d.ring * (sizeof(double) + sizeof(int2));

@@ -42,6 +42,52 @@ def test_chain_dp_matches_reference_golden(chaining):
         assert np.array_equal(p, g["dp_parent"][s:e]), c
 
 
+@pytest.mark.parametrize("lb", [1, 2, 31, 32, 33, 64, 65, 96, 97, 128, 160, 192, 224, 225, 300, 1024])
+def test_chain_dp_every_window_width_matches_oracle(chaining, lb):
+    """Window widths on both sides of every 32-anchor block boundary (the
+    broadcast form keeps ceil(lb/32)+1 blocks in registers up to 224, the
+    shared-memory ring form takes wider windows).  Dense anchors so that most
+    of the window is a valid predecessor; integer and fractional weights,
+    with and without a bonus; collinear runs for ties.  Bit patterns against
+    the oracle."""
+    from oracle import oracle
+
+    from graphmambaformer_b200.config import ChainingConfig
+
+    rng = np.random.default_rng(1000 + lb)
+    cfg = ChainingConfig(max_lookback=lb, max_gap=400)
+    lut = oracle.penalty_lut(400, cfg.gap_open, cfg.gap_extend, cfg.log_coeff)
+    for n, frac, with_bonus in ((1, False, False), (33, False, True), (700, False, False),
+                                (257, True, True), (96, False, False)):
+        if n == 96:  # collinear: equal candidates from many predecessors
+            re = np.repeat(np.arange(1, 49) * 7, 2)[:n].astype(np.int64)
+            fe = re.copy()
+        else:
+            re = np.sort(rng.integers(1, 4 * n + 2, size=n)).astype(np.int64)
+            fe = np.sort(rng.integers(1, 4 * n + 2, size=n)).astype(np.int64)
+        w = rng.integers(5, 30, size=n).astype(np.float64)
+        if frac:
+            w += rng.random(n)
+        bonus = rng.normal(0, 3, size=(n, lb)) if with_bonus else None
+        f, p = chaining.chain_dp_rows(re, fe, w, cfg, bonus=bonus)
+        ef, ep = oracle.chain_dp(re, fe, w, lut, lb, 400, bonus=bonus)
+        assert _same_bits(f, ef), (lb, n)
+        assert np.array_equal(p, ep), (lb, n)
+        assert n < 200 or lb < 2 or (p >= 0).mean() > 0.5, "the case must chain most anchors"
+    # a collinear run whose members sit the whole window apart, the anchors
+    # between them ahead on the read (never a valid predecessor of the run)
+    m = min(lb, 390)
+    i = np.arange(600)
+    run = i % m == 0
+    re = np.where(run, i + 1, 1_000_000 + i).astype(np.int64)
+    fe = (i + 1).astype(np.int64)
+    w = np.full(600, 15.0)
+    f, p = chaining.chain_dp_rows(re, fe, w, cfg)
+    ef, ep = oracle.chain_dp(re, fe, w, lut, lb, 400)
+    assert _same_bits(f, ef) and np.array_equal(p, ep), lb
+    assert np.array_equal(p[run][1:], i[run][1:] - m)
+
+
 def test_chain_dp_padded_known_answer(chaining):
     """tests/test_accel.py L347-370 of the reference, through the (B, A, 3)
     RawKernel signature; fractional weights, exact float64."""
