@@ -297,39 +297,51 @@ __global__ void __launch_bounds__(128) chain_dp_kernel(DpArgs a) {
 // strictly larger, so the first maximum (lowest j) wins as in the reference;
 // each candidate is the same float64 add / subtract.  After 32 steps the
 // finished block is stored (coalesced) and the next block is loaded.
+template <bool WEIGHT>
 __device__ __forceinline__ void dp_load_slot(const DpArgs& a, int64_t st, int64_t r0, int i, int n,
-                                             int& q, int& r, double& w) {
+                                             int& q, int& r, double& w, int& wl) {
     if (i < n) {
         const int64_t gi = st + i;
         q = a.read_end[gi];
         r = a.ref_end[gi];
-        w = a.weight ? a.weight[gi] : (double)a.length[r0 + a.perm[gi]];
+        if (WEIGHT) {
+            w = a.weight[gi];
+        } else {
+            wl = a.length[r0 + a.perm[gi]];
+            w = (double)wl;
+        }
     } else {
         q = 0;
         r = 0;
         w = 0.0;
+        wl = 0;
     }
 }
 
-template <int K>
+// Every candidate of a step is computed without branches (the table index is
+// clamped so that out-of-window pairs read in bounds) and folded in under one
+// predicate.  The running maxima start at -inf: the first valid candidate
+// (finite) always replaces it, as the reference's first maximum.
+template <int K, bool WEIGHT, bool BONUS>
 __global__ void __launch_bounds__(128) chain_dp_bcast_kernel(DpArgs a) {
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const int wpb = blockDim.x >> 5;
     const int lb = a.lookback > 1 ? a.lookback : 1;
     const unsigned mg = a.max_gap > 0 ? (unsigned)a.max_gap : 0u;
+    const double* __restrict__ lut = a.lut;
     for (int s = blockIdx.x * wpb + wib; s < a.n_segments; s += gridDim.x * wpb) {
         int64_t st;
         int n;
         seg_range(a, s, st, n);
         if (n <= 0) continue;
         const int64_t r0 = a.row_off ? 0 : a.read_off[s >> 1];
-        int q[K], rr[K], bj[K];
+        int q[K], rr[K], bj[K], wl[K];
         double w[K], best[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-            dp_load_slot(a, st, r0, 32 * k + lane, n, q[k], rr[k], w[k]);
-            best[k] = -DBL_MAX;
+            dp_load_slot<WEIGHT>(a, st, r0, 32 * k + lane, n, q[k], rr[k], w[k], wl[k]);
+            best[k] = -INFINITY;
             bj[k] = -1;
         }
         for (int base = 0; base < n; base += 32) {
@@ -338,34 +350,44 @@ __global__ void __launch_bounds__(128) chain_dp_bcast_kernel(DpArgs a) {
 #pragma unroll
             for (int k = 0; k < K; ++k) live[k] = base + 32 * k + lane < n;
             for (int u = 0; u < steps; ++u) {
-                const double fo = (bj[0] >= 0 && best[0] > w[0]) ? best[0] : w[0];
+                const double fo = best[0] > w[0] ? best[0] : w[0];
                 const double ft = __shfl_sync(FULL_MASK, fo, u);
                 const int qt = __shfl_sync(FULL_MASK, q[0], u);
                 const int rt = __shfl_sync(FULL_MASK, rr[0], u);
                 const int t = base + u;
+                const int lu = lane - u;
 #pragma unroll
                 for (int k = 0; k < K; ++k) {
-                    if (32 * k - u > lb) break;  // no anchor of this block reaches back to t
-                    const int d = 32 * k + lane - u;
+                    // a block none of whose anchors reaches back to t is skipped
+                    if (32 * k - u > lb) continue;
+                    const int d = 32 * k + lu;
                     const int dq = q[k] - qt;
                     const int dr = rr[k] - rt;
-                    if (live[k] && (unsigned)(d - 1) < (unsigned)lb && (unsigned)(dq - 1) < mg &&
-                        (unsigned)(dr - 1) < mg) {
-                        const double mn = (double)(dq < dr ? dq : dr);
-                        const double adv = mn < w[k] ? mn : w[k];
-                        const int gap = dr > dq ? dr - dq : dq - dr;
-                        double sc = __dsub_rn(__dadd_rn(ft, adv), __ldg(&a.lut[gap]));
-                        if (a.bonus)
-                            sc = __dadd_rn(sc, __ldg(&a.bonus[(st + base + 32 * k + lane) * lb + (lb - d)]));
-                        if (bj[k] < 0 || sc > best[k]) {
-                            best[k] = sc;
-                            bj[k] = t;
-                        }
+                    const bool ok = live[k] && (unsigned)(d - 1) < (unsigned)lb &&
+                                    (unsigned)(dq - 1) < mg && (unsigned)(dr - 1) < mg;
+                    const int mn = dq < dr ? dq : dr;
+                    double adv;
+                    if (WEIGHT) {
+                        const double mnd = (double)mn;
+                        adv = mnd < w[k] ? mnd : w[k];
+                    } else {
+                        adv = (double)(mn < wl[k] ? mn : wl[k]);
+                    }
+                    unsigned gap = (unsigned)(dr > dq ? dr - dq : dq - dr);
+                    gap = gap < mg ? gap : mg;
+                    double sc = __dsub_rn(__dadd_rn(ft, adv), __ldg(&lut[gap]));
+                    if (BONUS) {
+                        const int64_t bi = ok ? (st + base + 32 * k + lane) * lb + (lb - d) : 0;
+                        sc = __dadd_rn(sc, __ldg(&a.bonus[bi]));
+                    }
+                    if (ok && sc > best[k]) {
+                        best[k] = sc;
+                        bj[k] = t;
                     }
                 }
             }
             if (live[0]) {
-                const bool take = bj[0] >= 0 && best[0] > w[0];
+                const bool take = best[0] > w[0];
                 a.f[st + base + lane] = take ? best[0] : w[0];
                 a.parent[st + base + lane] = take ? bj[0] : -1;
             }
@@ -374,11 +396,12 @@ __global__ void __launch_bounds__(128) chain_dp_bcast_kernel(DpArgs a) {
                 q[k] = q[k + 1];
                 rr[k] = rr[k + 1];
                 w[k] = w[k + 1];
+                wl[k] = wl[k + 1];
                 best[k] = best[k + 1];
                 bj[k] = bj[k + 1];
             }
-            dp_load_slot(a, st, r0, base + 32 * K + lane, n, q[K - 1], rr[K - 1], w[K - 1]);
-            best[K - 1] = -DBL_MAX;
+            dp_load_slot<WEIGHT>(a, st, r0, base + 32 * K + lane, n, q[K - 1], rr[K - 1], w[K - 1], wl[K - 1]);
+            best[K - 1] = -INFINITY;
             bj[K - 1] = -1;
         }
     }
@@ -774,7 +797,16 @@ template <int K>
 int launch_dp_bcast(const DpArgs& d, int n_segments, cudaStream_t stream) {
     const int wpb = 4;
     const int blocks = (n_segments + wpb - 1) / wpb;
-    if (blocks > 0) chain_dp_bcast_kernel<K><<<blocks, 32 * wpb, 0, stream>>>(d);
+    if (blocks > 0) {
+        if (d.weight && d.bonus)
+            chain_dp_bcast_kernel<K, true, true><<<blocks, 32 * wpb, 0, stream>>>(d);
+        else if (d.weight)
+            chain_dp_bcast_kernel<K, true, false><<<blocks, 32 * wpb, 0, stream>>>(d);
+        else if (d.bonus)
+            chain_dp_bcast_kernel<K, false, true><<<blocks, 32 * wpb, 0, stream>>>(d);
+        else
+            chain_dp_bcast_kernel<K, false, false><<<blocks, 32 * wpb, 0, stream>>>(d);
+    }
     return cuda_status(cudaGetLastError());
 }
 

@@ -181,6 +181,30 @@ def test_chain_batch_matches_oracle_hifi_workload(chaining):
             assert np.array_equal(a.anchor_idx, b["anchor_idx"])
 
 
+@pytest.mark.parametrize("lb", [1, 16, 32, 96, 128, 160, 192, 224, 256])
+def test_chain_batch_every_window_width_matches_oracle(chaining, lb):
+    """The read-batch path (anchor lengths as weights) at window widths that
+    select each register-block count of the broadcast DP, and the ring form
+    beyond 224."""
+    from graphmambaformer_b200 import synth
+    from graphmambaformer_b200.config import ChainingConfig
+    from oracle import oracle
+
+    batch = synth.chaining_reads_hifi(n_reads=24, seed=40 + lb, ref_len=2_000_000, mean_len=6000)
+    cfg = ChainingConfig(max_lookback=lb, max_gap=5000)
+    got = chaining.chain_anchor_batch(batch, cfg)
+    want = oracle.chain_batch(batch.read_off, batch.read_pos, batch.ref_pos, batch.length,
+                              batch.strand, oracle.penalty_lut(5000, 6.0, 0.05, 0.5), max_lookback=lb,
+                              threads=8)
+    assert np.array_equal(got.n_chains, want.n_chains)
+    for r in range(len(batch)):
+        for a, b in zip(got.chains(r), want.chains(batch.read_off, r)):
+            assert a.score == b["score"] and a.is_primary == b["is_primary"]
+            assert [a.read_start, a.read_end, a.ref_start, a.ref_end] == [
+                b["read_start"], b["read_end"], b["ref_start"], b["ref_end"]]
+            assert np.array_equal(a.anchor_idx, b["anchor_idx"])
+
+
 def test_chain_batch_long_reads_wide_window(chaining):
     """ONT-like long reads (~10k anchors per read), lookback 200."""
     from graphmambaformer_b200 import synth
