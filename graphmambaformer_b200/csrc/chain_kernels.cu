@@ -502,9 +502,12 @@ __global__ void __launch_bounds__(256) chain_peel_kernel(PeelArgs a) {
         const int np2 = next_pow2(ns);
         unsigned long long* key;
         int* idx;
-        if (np2 <= a.smem_elems) {
+        // shared buffer of 12 * smem_elems bytes: keys from the bottom, the
+        // sorted indices at the top (they outlive the keys: the walk reads them)
+        const bool sort_smem = np2 <= a.smem_elems;
+        if (sort_smem) {
             key = pk_smem;
-            idx = reinterpret_cast<int*>(pk_smem + a.smem_elems);
+            idx = reinterpret_cast<int*>(reinterpret_cast<char*>(pk_smem) + 12 * a.smem_elems - 4 * np2);
         } else {
             key = a.gkey + 2 * a0;  // np2 <= 2n entries of this read's range
             idx = a.gidx + 2 * a0;
@@ -538,12 +541,12 @@ __global__ void __launch_bounds__(256) chain_peel_kernel(PeelArgs a) {
         // block.  The strand's walks claim all n nodes, so its members fill
         // mem_tmp[mem_base, mem_base + n).
         const int mem_base = n_memtot;
-        if (n <= a.smem_elems) {
+        if (6 * n + (sort_smem ? 4 * np2 : 0) <= 12 * a.smem_elems) {
             // shared memory, in the dead sort keys below the sorted starts:
             // pw[x] = predecessor + 1 with bit 31 set once claimed (one load
-            // per step of a walk), and the member list
+            // per step of a walk), and the member list (16-bit: n <= 4,096)
             int* pw = reinterpret_cast<int*>(pk_smem);
-            int* ml = pw + n;
+            unsigned short* ml = reinterpret_cast<unsigned short*>(pw + n);
             for (int x = threadIdx.x; x < n; x += blockDim.x) pw[x] = par[x] + 1;
             __syncthreads();
             if (threadIdx.x == 0) {
@@ -558,7 +561,7 @@ __global__ void __launch_bounds__(256) chain_peel_kernel(PeelArgs a) {
                     int node = i;
                     do {
                         pw[node] = v | (int)0x80000000u;
-                        ml[mo + m] = node;
+                        ml[mo + m] = (unsigned short)node;
                         ++m;
                         node = v - 1;
                         if (node < 0) break;
@@ -572,7 +575,7 @@ __global__ void __launch_bounds__(256) chain_peel_kernel(PeelArgs a) {
                 n_walk = w;
             }
             __syncthreads();
-            for (int x = threadIdx.x; x < n; x += blockDim.x) a.mem_tmp[a0 + mem_base + x] = ml[x];
+            for (int x = threadIdx.x; x < n; x += blockDim.x) a.mem_tmp[a0 + mem_base + x] = (int)ml[x];
         } else {
             int8_t* claimed = a.claimed + a0;  // held the dom flags
             for (int x = threadIdx.x; x < n; x += blockDim.x) claimed[x] = 0;
@@ -680,7 +683,7 @@ __global__ void __launch_bounds__(256) chain_peel_kernel(PeelArgs a) {
     int* idx;
     if (np2 <= a.smem_elems) {
         key = pk_smem;
-        idx = reinterpret_cast<int*>(pk_smem + a.smem_elems);
+        idx = reinterpret_cast<int*>(reinterpret_cast<char*>(pk_smem) + 12 * a.smem_elems - 4 * np2);
     } else {
         key = a.gkey + 2 * a0;
         idx = a.gidx + 2 * a0;
@@ -759,10 +762,12 @@ using namespace gmf;
 namespace {
 
 // Shared-memory sort buffers: 4096 keys (48 KB) for the per-read sort and
-// 2048 (24 KB) for the per-strand peel, so 4 and 9 CTAs fit an SM; larger
-// reads / strands sort in their own workspace range instead.
+// 2048 (24 KB) for the per-strand peel, so 4 and 8 CTAs fit an SM (the peel's
+// serial walk runs in 8 blocks per SM); larger reads / strands sort in their
+// own workspace range instead.  The peel buffer also holds a strand's walk
+// state (6 bytes per anchor) beside its sorted starts.
 int sort_smem_elems() { return 4096; }
-int peel_smem_elems() { return 4096; }
+int peel_smem_elems() { return 2048; }
 
 size_t sort_smem_bytes(int elems) { return (size_t)elems * (sizeof(unsigned long long) + sizeof(int)); }
 
