@@ -38,27 +38,51 @@ __device__ __forceinline__ bool pair_less(unsigned long long ka, int ia, unsigne
     return ka < kb || (ka == kb && ia < ib);
 }
 
+__device__ __forceinline__ void bitonic_pair(unsigned long long* key, int* idx, int x, int j, int k) {
+    const int y = x | j;  // x has bit j clear
+    const bool up = (x & k) == 0;
+    const unsigned long long kx = key[x], ky = key[y];
+    const int ix = idx[x], iy = idx[y];
+    const bool swap = up ? pair_less(ky, iy, kx, ix) : pair_less(kx, ix, ky, iy);
+    if (swap) {
+        key[x] = ky;
+        key[y] = kx;
+        idx[x] = iy;
+        idx[y] = ix;
+    }
+}
+
+// Threads take compare-exchange pairs (the p-th index with bit j clear and
+// its partner), not elements, so no lane idles.  Stages whose pairs stay
+// inside one warp's chunk of the array (j < chunk) need only __syncwarp; only
+// the widest strides synchronise the block.  Ends with __syncthreads.
 __device__ void block_bitonic(unsigned long long* key, int* idx, int npow2) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int ch = npow2 / nw;
+    if (ch < 64) ch = 64;
+    if (ch > npow2) ch = npow2;
+    const int n_chunks = npow2 / ch;
+    bool block_synced = true;
     for (int k = 2; k <= npow2; k <<= 1) {
         for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int x = threadIdx.x; x < npow2; x += blockDim.x) {
-                const int y = x ^ j;
-                if (y > x) {
-                    const bool up = (x & k) == 0;
-                    const unsigned long long kx = key[x], ky = key[y];
-                    const int ix = idx[x], iy = idx[y];
-                    const bool swap = up ? pair_less(ky, iy, kx, ix) : pair_less(kx, ix, ky, iy);
-                    if (swap) {
-                        key[x] = ky;
-                        key[y] = kx;
-                        idx[x] = iy;
-                        idx[y] = ix;
-                    }
+            if (j >= ch) {
+                if (!block_synced) __syncthreads();
+                for (int p = threadIdx.x; p < (npow2 >> 1); p += blockDim.x)
+                    bitonic_pair(key, idx, ((p & ~(j - 1)) << 1) | (p & (j - 1)), j, k);
+                __syncthreads();
+                block_synced = true;
+            } else {
+                for (int c = wid; c < n_chunks; c += nw) {
+                    const int base = c * ch;
+                    for (int p = lane; p < (ch >> 1); p += 32)
+                        bitonic_pair(key, idx, base + (((p & ~(j - 1)) << 1) | (p & (j - 1))), j, k);
                 }
+                __syncwarp();
+                block_synced = false;
             }
-            __syncthreads();
         }
     }
+    __syncthreads();
 }
 
 __host__ __device__ inline int next_pow2(int n) {
@@ -447,7 +471,7 @@ struct PeelArgs {
     int32_t* members;
 };
 
-__global__ void __launch_bounds__(256) chain_peel_kernel(PeelArgs a) {
+__global__ void __launch_bounds__(128) chain_peel_kernel(PeelArgs a) {
     extern __shared__ unsigned long long pk_smem[];
     const int r = blockIdx.x;
     if (r >= a.n_reads) return;
@@ -762,10 +786,10 @@ using namespace gmf;
 namespace {
 
 // Shared-memory sort buffers: 4096 keys (48 KB) for the per-read sort and
-// 2048 (24 KB) for the per-strand peel, so 4 and 8 CTAs fit an SM (the peel's
-// serial walk runs in 8 blocks per SM); larger reads / strands sort in their
-// own workspace range instead.  The peel buffer also holds a strand's walk
-// state (6 bytes per anchor) beside its sorted starts.
+// 2048 (24 KB) for the per-strand peel, so 4 and 9 CTAs fit an SM (the peel's
+// serial walk runs in 9 blocks of 4 warps per SM); larger reads / strands
+// sort in their own workspace range instead.  The peel buffer also holds a
+// strand's walk state (6 bytes per anchor) beside its sorted starts.
 int sort_smem_elems() { return 4096; }
 int peel_smem_elems() { return 2048; }
 
@@ -1042,7 +1066,7 @@ extern "C" int gmf_chain_batch(const gmf_anchor_batch* an, const gmf_chain_param
     const size_t smem = sort_smem_bytes(k.smem_elems);
     GMF_CUDA_TRY(cudaFuncSetAttribute(chain_peel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
-    chain_peel_kernel<<<an->n_reads, 256, smem, stream>>>(k);
+    chain_peel_kernel<<<an->n_reads, 128, smem, stream>>>(k);
     return cuda_status(cudaGetLastError());
 }
 
