@@ -354,7 +354,17 @@ __global__ void __launch_bounds__(128) chain_dp_bcast_kernel(DpArgs a) {
     const int lb = a.lookback > 1 ? a.lookback : 1;
     const unsigned mg = a.max_gap > 0 ? (unsigned)a.max_gap : 0u;
     const double* __restrict__ lut = a.lut;
-    for (int s = blockIdx.x * wpb + wib; s < a.n_segments; s += gridDim.x * wpb) {
+    // reads mode: warps take every read's longer strand first, then the
+    // shorter ones, so a block's warps have similar work and the short
+    // segments fill the tail
+    const int n_reads = a.n_segments >> 1;
+    for (int g = blockIdx.x * wpb + wib; g < a.n_segments; g += gridDim.x * wpb) {
+        int s = g;
+        if (!a.row_off) {
+            const int r = g < n_reads ? g : g - n_reads;
+            const int minus_longer = a.n_minus[r] > a.n_plus[r] ? 1 : 0;
+            s = 2 * r + (g < n_reads ? minus_longer : 1 - minus_longer);
+        }
         int64_t st;
         int n;
         seg_range(a, s, st, n);
