@@ -56,7 +56,7 @@ __device__ __forceinline__ void bitonic_pair(unsigned long long* key, int* idx, 
 // its partner), not elements, so no lane idles.  Stages whose pairs stay
 // inside one warp's chunk of the array (j < chunk) need only __syncwarp; only
 // the widest strides synchronise the block.  Ends with __syncthreads.
-__device__ void block_bitonic(unsigned long long* key, int* idx, int npow2) {
+__device__ __forceinline__ void block_bitonic(unsigned long long* key, int* idx, int npow2) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     int ch = npow2 / nw;
     if (ch < 64) ch = 64;
@@ -175,7 +175,11 @@ __global__ void __launch_bounds__(256) chain_sort_kernel(SortArgs a) {
         idx[x] = ix;
     }
     __syncthreads();
-    block_bitonic(key, idx, np2);
+    // the shared-memory call is spelled out so the sort uses shared loads
+    if (np2 <= a.smem_elems)
+        block_bitonic(sm_keys, reinterpret_cast<int*>(sm_keys + a.smem_elems), np2);
+    else
+        block_bitonic(key, idx, np2);
     const int m = cnt[0] + cnt[1];
     for (int x = threadIdx.x; x < m; x += blockDim.x) {
         const unsigned long long k = key[x];
@@ -565,7 +569,12 @@ __global__ void __launch_bounds__(128) chain_peel_kernel(PeelArgs a) {
             idx[x] = 0x7fffffff;
         }
         __syncthreads();
-        block_bitonic(key, idx, np2);
+        if (sort_smem)
+            block_bitonic(pk_smem,
+                          reinterpret_cast<int*>(reinterpret_cast<char*>(pk_smem) + 12 * a.smem_elems - 4 * np2),
+                          np2);
+        else
+            block_bitonic(key, idx, np2);
         __syncthreads();
         const int c_first = n_cand;  // chains found in earlier segments
         // The walk is serial in rank order (the reference's loop): one thread
@@ -685,6 +694,7 @@ __global__ void __launch_bounds__(128) chain_peel_kernel(PeelArgs a) {
             for (int c = c_first + wid; c < n_cand; c += nw) {
                 const int2 cm = a.c_mem[a0 + c];
                 int rs = 0x7fffffff, re = -0x7fffffff - 1, fs = 0x7fffffff, fe = -0x7fffffff - 1;
+#pragma unroll 4
                 for (int x = lane; x < cm.y; x += 32) {
                     const int o = a.perm[a0 + s0 + a.mem_tmp[a0 + cm.x + x]];
                     const int rp = a.read_pos[a0 + o], fp = a.ref_pos[a0 + o], ln = a.length[a0 + o];
@@ -732,7 +742,12 @@ __global__ void __launch_bounds__(128) chain_peel_kernel(PeelArgs a) {
         }
     }
     __syncthreads();
-    block_bitonic(key, idx, np2);
+    if (np2 <= a.smem_elems)
+        block_bitonic(pk_smem,
+                      reinterpret_cast<int*>(reinterpret_cast<char*>(pk_smem) + 12 * a.smem_elems - 4 * np2),
+                      np2);
+    else
+        block_bitonic(key, idx, np2);
     __shared__ int kept_c[64];
     __shared__ int n_kept;
     if (threadIdx.x == 0) {
@@ -780,9 +795,22 @@ __global__ void __launch_bounds__(128) chain_peel_kernel(PeelArgs a) {
             a.n_members[slot] = cm.y;
         }
         // the walk stored members from chain end to start: reverse to read order
-        for (int x = threadIdx.x; x < cm.y; x += blockDim.x) {
-            const int loc = a.mem_tmp[a0 + cm.x + (cm.y - 1 - x)];
-            a.members[a0 + wpos + x] = a.perm[a0 + s0 + loc];
+        // four members per thread per round: their loads are issued together
+        for (int x0 = threadIdx.x; x0 < cm.y; x0 += 4 * blockDim.x) {
+            int loc[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int x = x0 + u * blockDim.x;
+                loc[u] = x < cm.y ? a.mem_tmp[a0 + cm.x + (cm.y - 1 - x)] : 0;
+            }
+            int o[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) o[u] = x0 + u * blockDim.x < cm.y ? a.perm[a0 + s0 + loc[u]] : 0;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int x = x0 + u * blockDim.x;
+                if (x < cm.y) a.members[a0 + wpos + x] = o[u];
+            }
         }
         wpos += cm.y;
     }
