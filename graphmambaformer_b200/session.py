@@ -58,6 +58,9 @@ class _Buffers:
     def device_buf(self, name: str, n: int, dtype) -> torch.Tensor:
         return self._grow(self.dev, name, n, dtype, False)
 
+    def host_buf(self, name: str, n: int, dtype) -> torch.Tensor:
+        return self._grow(self.host, name, n, dtype, True)
+
     def download(self, name: str, d: torch.Tensor, n: int, stream) -> torch.Tensor:
         h = self._grow(self.host, name, n, d.dtype, True)
         if n:
@@ -176,51 +179,105 @@ class ChainSession:
                             self.cfg.log_coeff)
         self.h2d_bytes = 0
         self.d2h_bytes = 0
+        self._events: list = []
 
-    def chain(self, batch) -> ChainResult:
+    def chain(self, batch, chunks: Optional[int] = None) -> ChainResult:
+        """Chain a host batch.  Large batches go through in ``chunks`` runs of
+        whole reads (default: one per ~2 M anchors, at most 4) on the session
+        stream: while the device chains one run, the host stages the next run's
+        inputs and copies out the previous run's chains.  Reads are chained
+        independently, so the result does not depend on the split."""
         a = AnchorCSR.of(batch)
         R, A = len(a), int(a.read_off[-1])
         if R and np.diff(a.read_off).max() > _native.MAX_READ_ANCHORS:
             raise ValueError(f"a read has more than {_native.MAX_READ_ANCHORS} anchors")
+        C = chunks if chunks is not None else min(4, max(1, A // 2_000_000))
+        C = max(1, min(int(C), max(R, 1)))
+        # run k covers reads [cut[k], cut[k+1]), about A / C anchors each
+        cut = np.unique(np.concatenate([[0], np.searchsorted(a.read_off[1:], np.linspace(0, A, C + 1)[1:-1]),
+                                        [R]])).astype(np.int64)
+        C = len(cut) - 1 if R else 1
+        if not R:
+            cut = np.array([0, 0], np.int64)
         s = self.stream
-        up = self.buf.upload
-        ro = up("ro", a.read_off, s)
-        rp = up("rp", a.read_pos, s)
-        fp = up("fp", a.ref_pos, s)
-        ln = up("ln", a.length, s)
-        st = up("st", a.strand, s)
-        self.h2d_bytes = int(a.read_off.nbytes + a.read_pos.nbytes + a.ref_pos.nbytes
-                             + a.length.nbytes + a.strand.nbytes)
         mc = self.cp.max_chains
-        db = self.buf.device_buf
+        hb, db = self.buf.host_buf, self.buf.device_buf
         nR, nA = max(R, 1), max(A, 1)
-        o = dict(n=db("n", nR, torch.int32), score=db("score", nR * mc, torch.float64),
-                 strand=db("strand", nR * mc, torch.int32), span=db("span", 4 * nR * mc, torch.int32),
-                 prim=db("prim", nR * mc, torch.int32), nmem=db("nmem", nR * mc, torch.int32),
-                 mem=db("mem", nA, torch.int32))
-        need = int(_native.lib().gmf_chain_workspace_bytes(R, A))
-        ws = db("ws", need, torch.uint8)
-        batch_c = _native.GmfAnchorBatch(R, ro.data_ptr(), rp.data_ptr(), fp.data_ptr(), ln.data_ptr(),
-                                         st.data_ptr())
-        res_c = _native.GmfChainResults(o["n"].data_ptr(), o["score"].data_ptr(), o["strand"].data_ptr(),
-                                        o["span"].data_ptr(), o["prim"].data_ptr(), o["nmem"].data_ptr(),
-                                        o["mem"].data_ptr())
+        inputs = dict(rp=(a.read_pos, torch.int32), fp=(a.ref_pos, torch.int32), ln=(a.length, torch.int32),
+                      st=(a.strand, torch.int8))
+        h_in = {k: hb(k, nA, dt) for k, (_, dt) in inputs.items()}
+        d_in = {k: db(k, nA, dt) for k, (_, dt) in inputs.items()}
+        h_ro, d_ro = hb("ro", nR + C, torch.int64), db("ro", nR + C, torch.int64)
+        sizes = dict(n=(1, torch.int32), score=(mc, torch.float64), strand=(mc, torch.int32),
+                     span=(4 * mc, torch.int32), prim=(mc, torch.int32), nmem=(mc, torch.int32))
+        d_out = {k: db(k, nR * w, dt) for k, (w, dt) in sizes.items()}
+        h_out = {k: hb("h_" + k, nR * w, dt) for k, (w, dt) in sizes.items()}
+        d_mem, h_mem = db("mem", nA, torch.int32), hb("h_mem", nA, torch.int32)
+        widest_r = int(np.diff(cut).max()) if R else 0
+        widest_a = int(max(a.read_off[cut[k + 1]] - a.read_off[cut[k]] for k in range(C))) if R else 0
+        need = int(_native.lib().gmf_chain_workspace_bytes(widest_r, widest_a))
+        ws = db("ws", max(need, 1), torch.uint8)
         sp = int(s.cuda_stream)
         bind(self.device, sp)
-        rc = _native.lib().gmf_chain_batch(ctypes.byref(batch_c), ctypes.byref(self.cp),
-                                           ctypes.c_void_p(self.lut.data_ptr()), self.lut.numel(), None,
-                                           None, None, ctypes.byref(res_c), ctypes.c_void_p(ws.data_ptr()),
-                                           need, ctypes.c_void_p(sp))
-        _native.check("gmf_chain_batch", rc)
-        dl = self.buf.download
-        sizes = dict(n=R, score=R * mc, strand=R * mc, span=4 * R * mc, prim=R * mc, nmem=R * mc, mem=A)
-        h = {k: dl("h_" + k, o[k], sizes[k], s) for k in sizes}
-        s.synchronize()
-        self.d2h_bytes = int(sum(h[k][: sizes[k]].numel() * h[k].element_size() for k in sizes))
-        return ChainResult(a.read_off, h["n"][:R].numpy().copy(),
-                           h["score"][: R * mc].numpy().reshape(R, mc).copy(),
-                           h["strand"][: R * mc].numpy().reshape(R, mc).copy(),
-                           h["span"][: 4 * R * mc].numpy().reshape(R, mc, 4).copy(),
-                           h["prim"][: R * mc].numpy().reshape(R, mc).copy(),
-                           h["nmem"][: R * mc].numpy().reshape(R, mc).copy(),
-                           h["mem"][:A].numpy().copy(), self.d2h_bytes)
+        while len(self._events) < C:
+            self._events.append(torch.cuda.Event())
+        out = dict(n=np.empty(R, np.int32), score=np.empty(R * mc, np.float64), strand=np.empty(R * mc, np.int32),
+                   span=np.empty(4 * R * mc, np.int32), prim=np.empty(R * mc, np.int32),
+                   nmem=np.empty(R * mc, np.int32))
+        members = np.empty(A, np.int32)
+        h2d = 0
+
+        def stage(k):
+            nonlocal h2d
+            r0, r1 = int(cut[k]), int(cut[k + 1])
+            a0, a1 = int(a.read_off[r0]), int(a.read_off[r1])
+            ro = h_ro[r0 + k: r1 + k + 1]
+            ro.copy_(torch.from_numpy(a.read_off[r0: r1 + 1] - a0))
+            with torch.cuda.stream(s):
+                d_ro[r0 + k: r1 + k + 1].copy_(ro, non_blocking=True)
+            h2d += ro.numel() * 8
+            for name, (arr, _) in inputs.items():
+                if a1 > a0:
+                    h_in[name][a0:a1].copy_(torch.from_numpy(arr[a0:a1]))
+                    with torch.cuda.stream(s):
+                        d_in[name][a0:a1].copy_(h_in[name][a0:a1], non_blocking=True)
+                    h2d += (a1 - a0) * arr.itemsize
+            batch_c = _native.GmfAnchorBatch(
+                r1 - r0, d_ro.data_ptr() + 8 * (r0 + k), d_in["rp"].data_ptr() + 4 * a0,
+                d_in["fp"].data_ptr() + 4 * a0, d_in["ln"].data_ptr() + 4 * a0, d_in["st"].data_ptr() + a0)
+            o = {name: d_out[name].data_ptr() + d_out[name].element_size() * w * r0
+                 for name, (w, _) in sizes.items()}
+            res_c = _native.GmfChainResults(o["n"], o["score"], o["strand"], o["span"], o["prim"], o["nmem"],
+                                            d_mem.data_ptr() + 4 * a0)
+            rc = _native.lib().gmf_chain_batch(ctypes.byref(batch_c), ctypes.byref(self.cp),
+                                               ctypes.c_void_p(self.lut.data_ptr()), self.lut.numel(), None,
+                                               None, None, ctypes.byref(res_c), ctypes.c_void_p(ws.data_ptr()),
+                                               need, ctypes.c_void_p(sp))
+            _native.check("gmf_chain_batch", rc)
+            with torch.cuda.stream(s):
+                for name, (w, _) in sizes.items():
+                    h_out[name][w * r0: w * r1].copy_(d_out[name][w * r0: w * r1], non_blocking=True)
+                h_mem[a0:a1].copy_(d_mem[a0:a1], non_blocking=True)
+                self._events[k].record(s)
+
+        def collect(k):
+            r0, r1 = int(cut[k]), int(cut[k + 1])
+            a0, a1 = int(a.read_off[r0]), int(a.read_off[r1])
+            self._events[k].synchronize()
+            # torch's host copies run on several threads
+            for name, (w, _) in sizes.items():
+                torch.from_numpy(out[name][w * r0: w * r1]).copy_(h_out[name][w * r0: w * r1])
+            torch.from_numpy(members[a0:a1]).copy_(h_mem[a0:a1])
+
+        # the host stages run k+1 before copying out run k
+        for k in range(C):
+            stage(k)
+            if k:
+                collect(k - 1)
+        collect(C - 1)
+        self.h2d_bytes = h2d
+        self.d2h_bytes = int(R * sum(w * torch.tensor([], dtype=dt).element_size() for w, dt in sizes.values())
+                             + A * 4)
+        return ChainResult(a.read_off, out["n"], out["score"].reshape(R, mc), out["strand"].reshape(R, mc),
+                           out["span"].reshape(R, mc, 4), out["prim"].reshape(R, mc),
+                           out["nmem"].reshape(R, mc), members, self.d2h_bytes)

@@ -273,3 +273,30 @@ def test_empty_reads_and_single_strand(chaining):
     out = chaining.AffineChainer(ChainingConfig()).chain_batch(sets)
     assert out[0] == []
     assert len(out[1]) == 1 and out[1][0].strand == -1 and list(out[1][0].anchor_idx) == [0, 1, 2]
+
+
+@pytest.mark.parametrize("chunks", [None, 1, 3, 7])
+def test_chain_session_host_batches_in_runs(chaining, chunks):
+    """The host-buffer session (the e2e path): a batch split into runs of
+    whole reads, staged and copied out while the previous run chains, gives
+    the oracle's chains; so does a second call reusing the buffers."""
+    from graphmambaformer_b200 import synth
+    from graphmambaformer_b200.config import ChainingConfig
+    from graphmambaformer_b200.session import ChainSession
+    from oracle import oracle
+
+    batch = synth.chaining_reads_hifi(n_reads=60, seed=77, ref_len=2_000_000, mean_len=5000)
+    cfg = ChainingConfig(max_lookback=50, max_gap=5000)
+    want = oracle.chain_batch(batch.read_off, batch.read_pos, batch.ref_pos, batch.length, batch.strand,
+                              oracle.penalty_lut(5000, 6.0, 0.05, 0.5), max_lookback=50, threads=8)
+    sess = ChainSession(cfg, "cuda:0")
+    for _ in range(2):
+        got = sess.chain(batch, chunks=chunks)
+        assert np.array_equal(got.n_chains, want.n_chains)
+        for r in range(len(batch)):
+            for a, b in zip(got.chains(r), want.chains(batch.read_off, r)):
+                assert a.score == b["score"] and a.is_primary == b["is_primary"]
+                assert [a.read_start, a.read_end, a.ref_start, a.ref_end] == [
+                    b["read_start"], b["read_end"], b["ref_start"], b["ref_end"]]
+                assert np.array_equal(a.anchor_idx, b["anchor_idx"])
+    assert sess.h2d_bytes > 0 and sess.d2h_bytes > 0
