@@ -467,12 +467,13 @@ struct PeelArgs {
     // workspace (per anchor, in the read's range)
     unsigned long long* gkey;  // 2 * n_anchors
     int* gidx;                 // 2 * n_anchors
-    int32_t* mem_tmp;          // candidate members (sorted-local indices)
-    double* c_score;           // candidate records
-    int4* c_span;
+    int32_t* mem_tmp;          // walk members (sorted-local indices), all walks
+    double* c_score;           // candidate records; during a strand's walk, c_mem /
+    int4* c_span;              // c_span hold every walk's (offset, count) / (start, stop)
     int2* c_mem;               // (member offset within read, count)
     int8_t* c_strand;
-    int8_t* claimed;           // per anchor
+    int8_t* claimed;           // per anchor: skipped-start flags, then (strands
+                               // beyond the shared buffer) claimed flags
     int smem_elems;
     int64_t cap;               // anchors the workspace arrays hold
     // results
