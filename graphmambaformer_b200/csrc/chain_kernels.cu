@@ -506,7 +506,7 @@ __global__ void __launch_bounds__(128) chain_peel_kernel(PeelArgs a) {
     __shared__ int n_start;
     __shared__ int n_fill;
     __shared__ int n_walk;
-    __shared__ int warp_cnt[32];
+    __shared__ int warp_cnt[4];
     for (int seg = 0; seg < 2; ++seg) {
         const int n = seg == 0 ? np : nm;
         const int s0 = seg == 0 ? 0 : np;  // offset of the segment inside the read
@@ -688,74 +688,149 @@ __global__ void __launch_bounds__(128) chain_peel_kernel(PeelArgs a) {
                 __syncthreads();
             }
         }
-        // spans of this segment's chains over their members' original
-        // coordinates: one warp per chain, members 32 at a time
-        {
-            const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-            for (int c = c_first + wid; c < n_cand; c += nw) {
-                const int2 cm = a.c_mem[a0 + c];
-                int rs = 0x7fffffff, re = -0x7fffffff - 1, fs = 0x7fffffff, fe = -0x7fffffff - 1;
-#pragma unroll 4
-                for (int x = lane; x < cm.y; x += 32) {
-                    const int o = a.perm[a0 + s0 + a.mem_tmp[a0 + cm.x + x]];
-                    const int rp = a.read_pos[a0 + o], fp = a.ref_pos[a0 + o], ln = a.length[a0 + o];
-                    rs = min(rs, rp);
-                    re = max(re, rp + ln);
-                    fs = min(fs, fp);
-                    fe = max(fe, fp + ln);
-                }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    rs = min(rs, __shfl_xor_sync(FULL_MASK, rs, o));
-                    re = max(re, __shfl_xor_sync(FULL_MASK, re, o));
-                    fs = min(fs, __shfl_xor_sync(FULL_MASK, fs, o));
-                    fe = max(fe, __shfl_xor_sync(FULL_MASK, fe, o));
-                }
-                if (lane == 0) a.c_span[a0 + c] = make_int4(rs, re, fs, fe);
-            }
-        }
         __syncthreads();
     }
     __syncthreads();
     // ---- select ----
+    // The reference sorts the candidates by score (stable) and scans them:
+    // the first is kept, and once a chain is kept the scan stops at the
+    // first score below cutoff = best * ratio.  Only the first maximum and
+    // the candidates at or above the cutoff can be visited before that stop
+    // (a scan that has kept nothing by then keeps nothing later either), so
+    // only they are sorted and only their spans are computed.
     const int nc = n_cand;
     if (nc == 0) {
         if (threadIdx.x == 0) a.n_chains[r] = 0;
         return;
     }
-    const int np2 = next_pow2(nc);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    __shared__ double red_s[4];  // one entry per warp (at most 128 threads)
+    __shared__ int red_i[4];
+    __shared__ int4 red_span[4];
+    {
+        double bs = -INFINITY;
+        int bi = 0x7fffffff;
+        for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+            const double sc = a.c_score[a0 + c];
+            if (sc > bs || (sc == bs && c < bi)) {
+                bs = sc;
+                bi = c;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double os = __shfl_xor_sync(FULL_MASK, bs, o);
+            const int oi = __shfl_xor_sync(FULL_MASK, bi, o);
+            if (os > bs || (os == bs && oi < bi)) {
+                bs = os;
+                bi = oi;
+            }
+        }
+        if (lane == 0) {
+            red_s[wid] = bs;
+            red_i[wid] = bi;
+        }
+        if (threadIdx.x == 0) {
+            n_start = 0;
+            n_fill = 0;
+        }
+    }
+    __syncthreads();
+    double best_sc = red_s[0];
+    int best_c = red_i[0];
+    for (int w = 1; w < nw; ++w) {
+        if (red_s[w] > best_sc || (red_s[w] == best_sc && red_i[w] < best_c)) {
+            best_sc = red_s[w];
+            best_c = red_i[w];
+        }
+    }
+    const double cutoff = best_sc * a.secondary_score_ratio;
+    for (int x0 = threadIdx.x & ~31; x0 < nc; x0 += blockDim.x) {
+        const int c = x0 + lane;
+        const bool in = c < nc && (c == best_c || a.c_score[a0 + c] >= cutoff);
+        const unsigned b = __ballot_sync(FULL_MASK, in);
+        if (lane == 0 && b) atomicAdd(&n_start, __popc(b));
+    }
+    __syncthreads();
+    const int ns = n_start;
+    const int np2 = next_pow2(ns);
+    const bool sel_smem = np2 <= a.smem_elems;
     unsigned long long* key;
     int* idx;
-    if (np2 <= a.smem_elems) {
+    if (sel_smem) {
         key = pk_smem;
         idx = reinterpret_cast<int*>(reinterpret_cast<char*>(pk_smem) + 12 * a.smem_elems - 4 * np2);
     } else {
         key = a.gkey + 2 * a0;
         idx = a.gidx + 2 * a0;
     }
-    for (int x = threadIdx.x; x < np2; x += blockDim.x) {
-        if (x < nc) {
-            key[x] = ~ordered_bits(a.c_score[a0 + x]);  // sorted(key=-score), stable
-            idx[x] = x;
-        } else {
-            key[x] = ~0ull;
-            idx[x] = 0x7fffffff;
+    for (int x0 = threadIdx.x & ~31; x0 < nc; x0 += blockDim.x) {
+        const int c = x0 + lane;
+        const double sc = c < nc ? a.c_score[a0 + c] : 0.0;
+        const bool in = c < nc && (c == best_c || sc >= cutoff);
+        const unsigned b = __ballot_sync(FULL_MASK, in);
+        int base = 0;
+        if (lane == 0 && b) base = atomicAdd(&n_fill, __popc(b));
+        base = __shfl_sync(FULL_MASK, base, 0);
+        if (in) {
+            const int slot = base + __popc(b & lt);
+            key[slot] = ~ordered_bits(sc);  // sorted(key=-score), stable
+            idx[slot] = c;
         }
     }
+    for (int x = ns + threadIdx.x; x < np2; x += blockDim.x) {
+        key[x] = ~0ull;
+        idx[x] = 0x7fffffff;
+    }
     __syncthreads();
-    if (np2 <= a.smem_elems)
+    if (sel_smem)
         block_bitonic(pk_smem,
                       reinterpret_cast<int*>(reinterpret_cast<char*>(pk_smem) + 12 * a.smem_elems - 4 * np2),
                       np2);
     else
         block_bitonic(key, idx, np2);
+    // spans of the sorted candidates over their members' original
+    // coordinates, one candidate at a time across the block
+    for (int k = 0; k < ns; ++k) {
+        const int c = idx[k];
+        const int2 cm = a.c_mem[a0 + c];
+        const int s0 = a.c_strand[a0 + c] == 1 ? 0 : np;
+        int rs = 0x7fffffff, re = -0x7fffffff - 1, fs = 0x7fffffff, fe = -0x7fffffff - 1;
+#pragma unroll 4
+        for (int x = threadIdx.x; x < cm.y; x += blockDim.x) {
+            const int o = a.perm[a0 + s0 + a.mem_tmp[a0 + cm.x + x]];
+            const int rp = a.read_pos[a0 + o], fp = a.ref_pos[a0 + o], ln = a.length[a0 + o];
+            rs = min(rs, rp);
+            re = max(re, rp + ln);
+            fs = min(fs, fp);
+            fe = max(fe, fp + ln);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            rs = min(rs, __shfl_xor_sync(FULL_MASK, rs, o));
+            re = max(re, __shfl_xor_sync(FULL_MASK, re, o));
+            fs = min(fs, __shfl_xor_sync(FULL_MASK, fs, o));
+            fe = max(fe, __shfl_xor_sync(FULL_MASK, fe, o));
+        }
+        if (lane == 0) red_span[wid] = make_int4(rs, re, fs, fe);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int4 sp = red_span[0];
+            for (int w = 1; w < nw; ++w) {
+                const int4 q = red_span[w];
+                sp = make_int4(min(sp.x, q.x), max(sp.y, q.y), min(sp.z, q.z), max(sp.w, q.w));
+            }
+            a.c_span[a0 + c] = sp;
+        }
+        __syncthreads();
+    }
     __shared__ int kept_c[64];
     __shared__ int n_kept;
     if (threadIdx.x == 0) {
         const int mc = a.max_chains < 64 ? a.max_chains : 64;
         int kept = 0;
-        const double cutoff = a.c_score[a0 + idx[0]] * a.secondary_score_ratio;
-        for (int k = 0; k < nc; ++k) {
+        for (int k = 0; k < ns; ++k) {
             const int c = idx[k];
             const double sc = a.c_score[a0 + c];
             if (sc < cutoff && kept) break;
@@ -825,8 +900,8 @@ using namespace gmf;
 namespace {
 
 // Shared-memory sort buffers: 4096 keys (48 KB) for the per-read sort and
-// 2048 (24 KB) for the per-strand peel, so 4 and 9 CTAs fit an SM (the peel's
-// serial walk runs in 9 blocks of 4 warps per SM); larger reads / strands
+// 2048 (24 KB) for the per-strand peel, so 4 and 8 CTAs fit an SM (the peel's
+// serial walk runs in 8 blocks of 4 warps per SM); larger reads / strands
 // sort in their own workspace range instead.  The peel buffer also holds a
 // strand's walk state (6 bytes per anchor) beside its sorted starts.
 int sort_smem_elems() { return 4096; }
