@@ -165,6 +165,21 @@ class ExtensionSession:
         return res
 
 
+def run_cuts(read_off: np.ndarray, chunks: Optional[int] = None) -> np.ndarray:
+    """Read boundaries of the runs a chain batch goes through: run k covers
+    reads [cut[k], cut[k+1]), about A / C anchors each, no run empty (a batch
+    without reads is one empty run).  ``chunks`` = C; by default one run per
+    ~2 M anchors, at most 4."""
+    read_off = np.asarray(read_off, np.int64)
+    R, A = len(read_off) - 1, int(read_off[-1])
+    if R <= 0:
+        return np.array([0, 0], np.int64)
+    C = chunks if chunks is not None else min(4, max(1, A // 2_000_000))
+    C = max(1, min(int(C), R))
+    inner = np.searchsorted(read_off, np.linspace(0, A, C + 1)[1:-1], side="left")
+    return np.unique(np.concatenate([[0], np.clip(inner, 0, R), [R]])).astype(np.int64)
+
+
 class ChainSession:
     """Repeated fast-mode chaining (sort, DP, peel, select) on host batches."""
 
@@ -191,14 +206,8 @@ class ChainSession:
         R, A = len(a), int(a.read_off[-1])
         if R and np.diff(a.read_off).max() > _native.MAX_READ_ANCHORS:
             raise ValueError(f"a read has more than {_native.MAX_READ_ANCHORS} anchors")
-        C = chunks if chunks is not None else min(4, max(1, A // 2_000_000))
-        C = max(1, min(int(C), max(R, 1)))
-        # run k covers reads [cut[k], cut[k+1]), about A / C anchors each
-        cut = np.unique(np.concatenate([[0], np.searchsorted(a.read_off[1:], np.linspace(0, A, C + 1)[1:-1]),
-                                        [R]])).astype(np.int64)
-        C = len(cut) - 1 if R else 1
-        if not R:
-            cut = np.array([0, 0], np.int64)
+        cut = run_cuts(a.read_off, chunks)
+        C = len(cut) - 1
         s = self.stream
         mc = self.cp.max_chains
         hb, db = self.buf.host_buf, self.buf.device_buf
