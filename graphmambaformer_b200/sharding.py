@@ -4,8 +4,8 @@ Pairs and reads are independent units, so the path shards with no exchange
 on the data path: every rank takes a longest-processing-time share of the
 units (cost = in-band DP cells for extension pairs, anchors for chaining
 reads), aligns it on its own GPU, and only timings (max over ranks) or, if a
-caller wants them, results cross ranks.  No collective, peer load or TMA
-multicast touches the alignment data.
+caller wants them, results cross ranks.  No collective and no load from
+another GPU's memory touches the alignment data.
 """
 
 from __future__ import annotations
