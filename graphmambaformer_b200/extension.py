@@ -483,15 +483,13 @@ class ExtensionEngine:
             results[r].append(ext)
         return results
 
-    def _extend_wfa(self, items) -> list:
-        """WFA mode (extension.py L643-730): each chain is aligned end to end
-        against the reference stretch its read-zero diagonal and net indel
-        imply; a chain beyond ``wfa_max_distance`` falls back to banded SW of
-        that chain alone.  The score is recomputed from the CIGAR with the
-        affine parameters."""
-        from .wfa import align_wfa_pairs
-
-        cfg = self.cfg
+    @staticmethod
+    def _wfa_windows(items):
+        """WFA-mode pairs (extension.py L654-663): the read (reverse
+        complemented for strand -1) against the reference from the chain's
+        read-zero diagonal, as long as the read plus the chain's net indel.
+        Returns queries, targets and (read index, chain index, window start,
+        read length) per pair."""
         qs, ts, meta = [], [], []
         for r, (forward, chains, anchors, ref_codes) in enumerate(items):
             if not chains:
@@ -506,6 +504,18 @@ class ExtensionEngine:
                 qs.append(codes)
                 ts.append(ref_codes[start:end])
                 meta.append((r, ci, start, read_len))
+        return qs, ts, meta
+
+    def _extend_wfa(self, items) -> list:
+        """WFA mode (extension.py L643-730): each chain is aligned end to end
+        against the reference stretch its read-zero diagonal and net indel
+        imply; a chain beyond ``wfa_max_distance`` falls back to banded SW of
+        that chain alone.  The score is recomputed from the CIGAR with the
+        affine parameters."""
+        from .wfa import align_wfa_pairs
+
+        cfg = self.cfg
+        qs, ts, meta = self._wfa_windows(items)
         results: list = [[None] * len(it[1]) for it in items]
         if not meta:
             return [[] for _ in items]
