@@ -13,6 +13,10 @@
  *                         arithmetic, -1e30 sentinels, exclusive cummax scan
  *                         for E, first-index row max, strict '>' best update,
  *                         per-pair x-drop)
+ *   oracle_sw_batch       the same with B > 1 per group: the group's row loop
+ *                         stops after the first row on which every member
+ *                         has dropped (L190-193); rows past a member's query
+ *                         are empty (in_band needs i <= qlen)
  *   oracle_traceback_pair extension.py L207-302 (traceback_banded: f64
  *                         comparisons with tolerance 1e-3, out-of-matrix
  *                         cells read as -1e30, diag > F > E priority)
@@ -61,9 +65,23 @@ typedef struct {
 /* H/E/F are (qlen+1) x W row-major, row 0 initialised like the reference    */
 /* (H zeros, E/F -1e30).  Returns the number of rows actually computed.     */
 /* ------------------------------------------------------------------------ */
+/* sw_rows: rows 1..min(qlen, max_rows); with own_xdrop the pair stops on   */
+/* its own x-drop; row_best (optional) receives each computed row's best.   */
+static int sw_rows(const int16_t* q, int32_t qlen, const int16_t* t, int32_t tlen, int32_t hb,
+                   int32_t off, const sw_params* p, int32_t max_rows, int own_xdrop, float* H,
+                   float* E, float* F, float* out_score, int64_t* out_qend, int64_t* out_tend,
+                   float* row_best_out);
+
 int oracle_sw_pair(const int16_t* q, int32_t qlen, const int16_t* t, int32_t tlen,
                    int32_t hb, int32_t off, const sw_params* p, float* H, float* E,
                    float* F, float* out_score, int64_t* out_qend, int64_t* out_tend) {
+    return sw_rows(q, qlen, t, tlen, hb, off, p, qlen, 1, H, E, F, out_score, out_qend, out_tend, NULL);
+}
+
+static int sw_rows(const int16_t* q, int32_t qlen, const int16_t* t, int32_t tlen, int32_t hb,
+                   int32_t off, const sw_params* p, int32_t max_rows, int own_xdrop, float* H,
+                   float* E, float* F, float* out_score, int64_t* out_qend, int64_t* out_tend,
+                   float* row_best_out) {
     const int W = 2 * hb + 1;
     const long rows = (long)qlen + 1;
     for (long k = 0; k < rows * W; ++k) {
@@ -90,7 +108,8 @@ int oracle_sw_pair(const int16_t* q, int32_t qlen, const int16_t* t, int32_t tle
     float best = 0.0f, seen = 0.0f;
     int64_t bi = 0, bj = 0;
     int computed = 0;
-    for (int i = 1; i <= qlen; ++i) {
+    const int32_t last = max_rows < qlen ? max_rows : qlen;
+    for (int i = 1; i <= last; ++i) {
         const int16_t qb = q[i - 1];
         for (int d = 0; d < W; ++d) {
             const long j = (long)i + off - hb + d;
@@ -145,7 +164,8 @@ int oracle_sw_pair(const int16_t* q, int32_t qlen, const int16_t* t, int32_t tle
         hprev[W] = 0.0f;
         fprev[W] = NEG_F32;
         computed = i;
-        if (p->x_drop > 0.0f && (seen - row_best) > p->x_drop) break;
+        if (row_best_out) row_best_out[i - 1] = row_best;
+        if (own_xdrop && p->x_drop > 0.0f && (seen - row_best) > p->x_drop) break;
     }
     *out_score = best;
     *out_qend = bi;
@@ -231,8 +251,13 @@ static long rle_reverse(const unsigned char* ops_rev, long n, uint32_t* out) {
 }
 
 /* ------------------------------------------------------------------------ */
-/* Batched driver: per pair SW + traceback, pthreads over pairs.            */
-/* cigar holds, for pair b, up to cigar_cap[b] words at cigar_off[b].       */
+/* Batched driver: SW + traceback, pthreads over x-drop groups.              */
+/* A group is one call of the reference's banded_affine_sw_batch            */
+/* (extension.py L78-204): its row loop stops only after the first row on   */
+/* which every member has dropped (L190-193), and a member past its own     */
+/* query length has an empty row (H = 0, row best 0).  group_off = NULL     */
+/* makes every pair its own group.  cigar holds, for pair b, up to          */
+/* cigar_cap[b] words at cigar_off[b].                                      */
 /* ------------------------------------------------------------------------ */
 typedef struct {
     int32_t n_pairs;
@@ -244,35 +269,33 @@ typedef struct {
     uint32_t* cigar; const int64_t* cigar_off; int32_t* cigar_n;
     int32_t* counts; /* 4 per pair: = X I D */
     int traceback;
-    int64_t next; /* work counter */
+    const int64_t* group_off; int32_t n_groups;
+    int64_t next; /* work counter (groups) */
     pthread_mutex_t lock;
     int status;
 } sw_job;
 
-static void* sw_worker(void* arg) {
-    sw_job* job = (sw_job*)arg;
-    for (;;) {
-        pthread_mutex_lock(&job->lock);
-        const int64_t b = job->next++;
-        pthread_mutex_unlock(&job->lock);
-        if (b >= job->n_pairs) break;
-        const int16_t* q = job->q + job->q_off[b];
-        const int32_t qlen = (int32_t)(job->q_off[b + 1] - job->q_off[b]);
-        const int16_t* t = job->t + job->t_off[b];
-        const int32_t tlen = (int32_t)(job->t_off[b + 1] - job->t_off[b]);
-        const int32_t hb = job->hb[b], off = job->off[b];
-        const int W = 2 * hb + 1;
-        const long rows = (long)qlen + 1;
-        float* H = (float*)malloc(sizeof(float) * rows * W);
-        float* E = (float*)malloc(sizeof(float) * rows * W);
-        float* F = (float*)malloc(sizeof(float) * rows * W);
-        if (!H || !E || !F) {
-            free(H); free(E); free(F);
-            job->status = -1;
-            continue;
-        }
-        float sc; int64_t qe, te;
-        oracle_sw_pair(q, qlen, t, tlen, hb, off, job->p, H, E, F, &sc, &qe, &te);
+/* One pair: rows 1..min(qlen, max_rows), its own x-drop stop if own_xdrop,  */
+/* then the traceback.  row_best: NULL, or one float per query row.         */
+static int sw_member(sw_job* job, int64_t b, int32_t max_rows, int own_xdrop, int outputs,
+                     float* row_best) {
+    const int16_t* q = job->q + job->q_off[b];
+    const int32_t qlen = (int32_t)(job->q_off[b + 1] - job->q_off[b]);
+    const int16_t* t = job->t + job->t_off[b];
+    const int32_t tlen = (int32_t)(job->t_off[b + 1] - job->t_off[b]);
+    const int32_t hb = job->hb[b], off = job->off[b];
+    const int W = 2 * hb + 1;
+    const long rows = (long)qlen + 1;
+    float* H = (float*)malloc(sizeof(float) * rows * W);
+    float* E = (float*)malloc(sizeof(float) * rows * W);
+    float* F = (float*)malloc(sizeof(float) * rows * W);
+    if (!H || !E || !F) {
+        free(H); free(E); free(F);
+        return -1;
+    }
+    float sc; int64_t qe, te;
+    sw_rows(q, qlen, t, tlen, hb, off, job->p, max_rows, own_xdrop, H, E, F, &sc, &qe, &te, row_best);
+    if (outputs) {
         job->score[b] = sc;
         job->q_end[b] = qe;
         job->t_end[b] = te;
@@ -289,7 +312,72 @@ static void* sw_worker(void* arg) {
             job->cigar_n[b] = (int32_t)rle_reverse(ops, n, job->cigar + job->cigar_off[b]);
             free(ops);
         }
-        free(H); free(E); free(F);
+    }
+    free(H); free(E); free(F);
+    return 0;
+}
+
+/* The row on which a group's loop stops: every member's rows without a stop, */
+/* then the first row where (running max of row bests) - row best > x_drop   */
+/* for all members.  Returns -1 when out of memory.                          */
+static int32_t group_stop_row(sw_job* job, int64_t lo, int64_t hi) {
+    int32_t maxq = 0;
+    for (int64_t b = lo; b < hi; ++b) {
+        const int32_t ql = (int32_t)(job->q_off[b + 1] - job->q_off[b]);
+        if (ql > maxq) maxq = ql;
+    }
+    if (maxq == 0) return 0;
+    const int64_t nm = hi - lo;
+    float* rb = (float*)calloc((size_t)nm * (size_t)maxq, sizeof(float));
+    float* seen = (float*)calloc((size_t)nm, sizeof(float));
+    if (!rb || !seen) {
+        free(rb); free(seen);
+        return -1;
+    }
+    for (int64_t b = lo; b < hi; ++b) {
+        const int32_t ql = (int32_t)(job->q_off[b + 1] - job->q_off[b]);
+        if (sw_member(job, b, ql, 0, 0, rb + (b - lo) * maxq) != 0) {
+            free(rb); free(seen);
+            return -1;
+        }
+    }
+    int32_t stop = maxq;
+    for (int32_t i = 0; i < maxq; ++i) {
+        int all = 1;
+        for (int64_t m = 0; m < nm; ++m) {
+            const float r = rb[m * maxq + i]; /* 0 past the member's query */
+            if (r > seen[m]) seen[m] = r;
+            if (!((seen[m] - r) > job->p->x_drop)) all = 0;
+        }
+        if (all) {
+            stop = i + 1;
+            break;
+        }
+    }
+    free(rb); free(seen);
+    return stop;
+}
+
+static void* sw_worker(void* arg) {
+    sw_job* job = (sw_job*)arg;
+    const int32_t n_groups = job->group_off ? job->n_groups : job->n_pairs;
+    for (;;) {
+        pthread_mutex_lock(&job->lock);
+        const int64_t g = job->next++;
+        pthread_mutex_unlock(&job->lock);
+        if (g >= n_groups) break;
+        const int64_t lo = job->group_off ? job->group_off[g] : g;
+        const int64_t hi = job->group_off ? job->group_off[g + 1] : g + 1;
+        const int grouped = (hi - lo > 1) && job->p->x_drop > 0.0f;
+        const int32_t stop = grouped ? group_stop_row(job, lo, hi) : 0;
+        if (stop < 0) {
+            job->status = -1;
+            continue;
+        }
+        for (int64_t b = lo; b < hi; ++b) {
+            const int32_t ql = (int32_t)(job->q_off[b + 1] - job->q_off[b]);
+            if (sw_member(job, b, grouped ? stop : ql, !grouped, 1, NULL) != 0) job->status = -1;
+        }
     }
     return NULL;
 }
@@ -299,9 +387,9 @@ int oracle_sw_batch(int32_t n_pairs, const int16_t* q, const int64_t* q_off, con
                     const sw_params* p, int32_t traceback, int32_t n_threads, float* score,
                     int64_t* q_end, int64_t* t_end, int64_t* q_start, int64_t* t_start,
                     uint32_t* cigar, const int64_t* cigar_off, int32_t* cigar_n,
-                    int32_t* counts) {
+                    int32_t* counts, const int64_t* group_off, int32_t n_groups) {
     sw_job job = {n_pairs, q, q_off, t, t_off, hb, off, p, score, q_end, t_end, q_start, t_start,
-                  cigar, cigar_off, cigar_n, counts, traceback, 0,
+                  cigar, cigar_off, cigar_n, counts, traceback, group_off, n_groups, 0,
                   PTHREAD_MUTEX_INITIALIZER, 0};
     if (n_threads < 1) n_threads = 1;
     pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * n_threads);

@@ -107,8 +107,11 @@ def sw_batch(
     x_drop: float = 600.0,
     traceback: bool = True,
     threads: int = 1,
+    group_off: Optional[Sequence[int]] = None,
 ) -> SWOut:
-    """Per-pair ``banded_affine_sw_batch`` (B=1) + ``traceback_banded``."""
+    """``banded_affine_sw_batch`` + ``traceback_banded``: per pair (B=1), or,
+    with ``group_off``, one reference batch per group of consecutive pairs
+    (pairs group_off[g] .. group_off[g+1]-1), whose x-drop stop is shared."""
     B = len(queries)
     hb = np.broadcast_to(np.asarray(half_band, dtype=np.int32), (B,)).copy()
     off = np.broadcast_to(np.asarray(band_offset, dtype=np.int32), (B,)).copy()
@@ -126,10 +129,16 @@ def sw_batch(
     cn = np.zeros(B, dtype=np.int32)
     counts = np.zeros((B, 4), dtype=np.int32)
     params = SWParams(match, mismatch, gap_open, gap_extend, x_drop)
+    g_off = None
+    if group_off is not None:
+        g_off = np.ascontiguousarray(group_off, dtype=np.int64)
+        if len(g_off) < 1 or g_off[0] != 0 or g_off[-1] != B or np.any(np.diff(g_off) < 0):
+            raise ValueError("group_off must rise from 0 to the number of pairs")
     status = lib().oracle_sw_batch(
         ctypes.c_int32(B), _p(q), _p(q_off), _p(t), _p(t_off), _p(hb), _p(off),
         ctypes.byref(params), ctypes.c_int32(1 if traceback else 0), ctypes.c_int32(threads),
         _p(score), _p(qe), _p(te), _p(qs), _p(ts), _p(cigar), _p(c_off), _p(cn), _p(counts),
+        None if g_off is None else _p(g_off), ctypes.c_int32(0 if g_off is None else len(g_off) - 1),
     )
     if status != 0:
         raise MemoryError("oracle_sw_batch could not allocate its DP matrices")
@@ -154,6 +163,11 @@ def sw_matrices(query: np.ndarray, target: np.ndarray, half_band: int, band_offs
     qe = ctypes.c_int64()
     te = ctypes.c_int64()
     params = SWParams(match, mismatch, gap_open, gap_extend, x_drop)
+    g_off = None
+    if group_off is not None:
+        g_off = np.ascontiguousarray(group_off, dtype=np.int64)
+        if len(g_off) < 1 or g_off[0] != 0 or g_off[-1] != B or np.any(np.diff(g_off) < 0):
+            raise ValueError("group_off must rise from 0 to the number of pairs")
     lib().oracle_sw_pair(
         _p(q if len(q) else np.zeros(1, np.int16)), ctypes.c_int32(len(q)),
         _p(t if len(t) else np.zeros(1, np.int16)), ctypes.c_int32(len(t)),

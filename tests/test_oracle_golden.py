@@ -168,3 +168,26 @@ def test_wfa_oracle_is_levenshtein():
         assert sum(n for op, n in cigar if op in "=XD") == len(b)
         if len(a) and len(b):
             assert sum(n for op, n in cigar if op in "XID") == d
+
+
+def test_grouped_sw_oracle_matches_reference_xdrop_golden(golden_dir):
+    """The batch x-drop rule (extension.py L190-193): each golden batch is one
+    group whose row loop stops together; ends, starts and CIGARs match the
+    reference's `banded_affine_sw_batch` + `traceback_banded`.  Without the
+    group, some pairs stop earlier and some results differ."""
+    g = _load(golden_dir, "xdrop_golden.npz")
+    differ = 0
+    for b in range(len(g["batch_off"]) - 1):
+        lo, hi = int(g["batch_off"][b]), int(g["batch_off"][b + 1])
+        qs = [g["query"][g["query_off"][p]: g["query_off"][p + 1]] for p in range(lo, hi)]
+        ts = [g["target"][g["target_off"][p]: g["target_off"][p + 1]] for p in range(lo, hi)]
+        args = (qs, ts, g["half_band"][lo:hi], g["band_offset"][lo:hi], 2.0, 4.0, 6.0, 2.0, float(g["x_drop"][b]))
+        out = oracle.sw_batch(*args, group_off=[0, hi - lo])
+        alone = oracle.sw_batch(*args)
+        for k, p in enumerate(range(lo, hi)):
+            assert (float(out.score[k]), int(out.query_end[k]), int(out.target_end[k])) == (
+                g["score"][p], g["qe"][p], g["te"][p]), p
+            assert (int(out.query_start[k]), int(out.target_start[k])) == (g["qs"][p], g["ts"][p]), p
+            assert out.cigars[k] == _words_to_cigar(g["cigar"][g["cigar_off"][p]: g["cigar_off"][p + 1]]), p
+            differ += (float(alone.score[k]), int(alone.query_end[k])) != (float(out.score[k]), int(out.query_end[k]))
+    assert differ > 0, "the fixture must contain pairs that the group keeps running"
