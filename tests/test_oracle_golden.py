@@ -191,3 +191,26 @@ def test_grouped_sw_oracle_matches_reference_xdrop_golden(golden_dir):
             assert out.cigars[k] == _words_to_cigar(g["cigar"][g["cigar_off"][p]: g["cigar_off"][p + 1]]), p
             differ += (float(alone.score[k]), int(alone.query_end[k])) != (float(out.score[k]), int(out.query_end[k]))
     assert differ > 0, "the fixture must contain pairs that the group keeps running"
+
+
+def test_grouped_sw_oracle_edges():
+    """Groups of one, x-drop off, and members with empty queries: the group
+    rule reduces to the per-pair one where it should, and a group stops no
+    later than its last member's query."""
+    rng = np.random.default_rng(11)
+    qs = [rng.integers(0, 4, int(n)).astype(np.int16) for n in rng.integers(0, 120, 12)]
+    qs[3] = np.zeros(0, np.int16)
+    ts = [np.concatenate([q, rng.integers(0, 4, 40).astype(np.int16)]) for q in qs]
+    hb, off = np.full(12, 16), np.zeros(12, np.int64)
+    for xd in (0.0, 5.0, 30.0):
+        alone = oracle.sw_batch(qs, ts, hb, off, 2, 4, 6, 2, xd)
+        ones = oracle.sw_batch(qs, ts, hb, off, 2, 4, 6, 2, xd, group_off=np.arange(13))
+        grouped = oracle.sw_batch(qs, ts, hb, off, 2, 4, 6, 2, xd, group_off=[0, 4, 12])
+        for k in range(12):
+            assert (ones.score[k], ones.query_end[k], ones.cigars[k]) == (
+                alone.score[k], alone.query_end[k], alone.cigars[k])
+            if xd == 0.0:
+                assert (grouped.score[k], grouped.query_end[k], grouped.cigars[k]) == (
+                    alone.score[k], alone.query_end[k], alone.cigars[k])
+            assert grouped.score[k] >= alone.score[k]  # a group only runs longer
+        assert grouped.score[3] == 0 and grouped.cigars[3] == []
