@@ -163,11 +163,6 @@ def sw_matrices(query: np.ndarray, target: np.ndarray, half_band: int, band_offs
     qe = ctypes.c_int64()
     te = ctypes.c_int64()
     params = SWParams(match, mismatch, gap_open, gap_extend, x_drop)
-    g_off = None
-    if group_off is not None:
-        g_off = np.ascontiguousarray(group_off, dtype=np.int64)
-        if len(g_off) < 1 or g_off[0] != 0 or g_off[-1] != B or np.any(np.diff(g_off) < 0):
-            raise ValueError("group_off must rise from 0 to the number of pairs")
     lib().oracle_sw_pair(
         _p(q if len(q) else np.zeros(1, np.int16)), ctypes.c_int32(len(q)),
         _p(t if len(t) else np.zeros(1, np.int16)), ctypes.c_int32(len(t)),

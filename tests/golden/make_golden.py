@@ -1,9 +1,9 @@
 """Generate golden vectors by running the reference implementation itself.
 
-Run in a container that has the reference checked out (read-only) at
-``$GMF_REFERENCE`` (default ``/root/reference``)::
+Run in a container that has the reference checked out (read-only), naming
+its root in ``$GMF_REFERENCE`` or with ``--reference PATH``::
 
-    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py
+    GMF_REFERENCE=<reference root> PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py [which ...]
 
 It imports ``graphmambaformer.alignment`` from the reference, feeds it seeded
 synthetic inputs, and stores inputs + outputs as small compressed ``.npz``
@@ -50,6 +50,11 @@ Fixtures:
 * ``hybrid_golden.pkl`` -- ``AffineChainer.chain`` with a ``ChainingContext``
   (graph-distance oracle, backbone bias, neural seed scores with each AGNES
   trust decision, learned transitions).
+* ``hybrid_inputs_golden.pkl`` -- the two hybrid-mode DP inputs alone,
+  ``AffineChainer._weights`` and ``AffineChainer._graph_bonus``, on strand-
+  sorted anchor segments over random graphs (several hop limits, lookbacks,
+  bonus weights, the legacy linear blend, duplicated anchor keys, transition
+  keys that are not in the segment).
 """
 
 from __future__ import annotations
@@ -59,7 +64,20 @@ import sys
 
 import numpy as np
 
-REF = os.environ.get("GMF_REFERENCE", "/root/reference")
+def _reference_root() -> str:
+    args = sys.argv[1:]
+    if "--reference" in args:
+        i = args.index("--reference")
+        root = args[i + 1]
+        del sys.argv[i + 1: i + 3]
+        return root
+    root = os.environ.get("GMF_REFERENCE")
+    if not root:
+        sys.exit("make_golden.py: name the reference checkout with $GMF_REFERENCE or --reference PATH")
+    return root
+
+
+REF = _reference_root()
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))  # repo root
 sys.path.insert(0, REF)
@@ -473,6 +491,81 @@ def make_hybrid(rng):
     with open(os.path.join(HERE, "hybrid_golden.pkl"), "wb") as fh:
         pickle.dump(payload, fh, protocol=4)
     print(f"hybrid_golden.pkl: {len(reads)} reads, {sum(len(c) for c in out)} chains")
+
+
+def make_hybrid_inputs(rng):
+    """The reference's hybrid-mode weight and bonus rows on strand-sorted
+    anchor segments: each case keeps the segment's columns, the context and
+    the config overrides, and the reference's outputs."""
+    import pickle
+    from dataclasses import replace
+
+    from graphmambaformer.alignment.chaining import ChainingContext, GraphDistanceOracle
+
+    graphs = []
+    for n_nodes, extra in ((50, 6), (400, 120), (1500, 40)):
+        chain = [[i, i + 1] for i in range(n_nodes - 1) if rng.random() < 0.92]  # some breaks: components
+        more = rng.integers(0, n_nodes, size=(extra, 2)).tolist()
+        edges = np.array(chain + more, dtype=np.int64).T
+        graphs.append((edges, n_nodes))
+    cases = []
+    for c in range(60):
+        edges, n_nodes = graphs[c % 3]
+        hops = int((2, 3, 4)[c % 3])
+        oracle = GraphDistanceOracle(edges, n_nodes, max_hops=hops)
+        n = int(rng.integers(1, 90))
+        rp = np.sort(rng.integers(0, 20_000, size=n)).astype(np.int64)
+        fp = (rp + 1000 + rng.integers(-40, 40, size=n)).astype(np.int64)
+        ln = rng.integers(10, 30, size=n).astype(np.int64)
+        strand = 1 if c % 2 else -1
+        if c % 7 == 3 and n > 4:  # duplicated anchor keys
+            rp[1], fp[1], ln[1] = rp[0], fp[0], ln[0]
+            rp[3], fp[3], ln[3] = rp[2], fp[2], ln[2]
+        nid = np.where(rng.random(n) < 0.85, rng.integers(0, n_nodes, size=n), -1).astype(np.int64)
+        a = AnchorSet.from_lists(rp, fp, ln, np.full(n, strand, np.int8), node_id=nid)
+        kind = c % 5
+        if kind == 0:
+            a.score = np.full(n, np.nan, np.float32)
+        elif kind == 1:
+            a.score = np.where(rng.random(n) < 0.75, 0.97, 0.02).astype(np.float32)
+        else:
+            sc = rng.random(n).astype(np.float32)
+            sc[rng.random(n) < 0.2] = np.nan
+            a.score = sc
+        sub, _ = a.for_strand(strand)
+        sub, _ = sub.sorted_by_ref()
+        trust = [None, True, False, True, None][c % 5]
+        trans = None
+        if trust is True:
+            keys = [(int(sub.read_pos[i]), int(sub.ref_pos[i]), int(sub.length[i]), int(sub.strand[i]))
+                    for i in range(len(sub))]
+            trans = {}
+            for i in range(len(sub)):
+                for j in rng.integers(max(0, i - 40), i + 1, size=3):
+                    if j < i:
+                        trans[(keys[int(j)], keys[i])] = float(rng.random())
+            trans[((-1, -1, 1, 1), keys[0])] = 0.5  # a key the segment does not have
+            if len(sub) > 2:
+                trans[(keys[0], keys[-1])] = float(rng.random())  # beyond most lookbacks
+        backbone = (rng.random(n_nodes) < 0.5) if c % 3 != 1 else None
+        ctx = ChainingContext(oracle=oracle if c % 4 != 2 else None, backbone=backbone, trust_neural=trust,
+                              learned_transitions=trans)
+        over = dict(max_lookback=int((1, 16, 50, 64, 7)[c % 5]),
+                    graph_bonus=float((4.0, 2.5, 0.0, 4.0, 1.25)[c % 5]),
+                    graph_max_hops=int((3, 2, 4, 1, 3)[c % 5]),
+                    adaptive_seed_scoring=c % 6 != 5)
+        cfg = replace(ChainingConfig(), **over)
+        chainer = AffineChainer(cfg, backend="torch", workers=1)
+        w = chainer._weights(sub, ctx)
+        b = chainer._graph_bonus(sub, ctx)
+        cases.append(dict(read_pos=sub.read_pos, ref_pos=sub.ref_pos, length=sub.length, strand=sub.strand,
+                          node_id=sub.node_id, score=sub.score, edges=edges, n_nodes=n_nodes, max_hops=hops,
+                          use_oracle=ctx.oracle is not None, backbone=backbone, trust=trust, transitions=trans,
+                          cfg=over, weight=w, bonus=b))
+    with open(os.path.join(HERE, "hybrid_inputs_golden.pkl"), "wb") as fh:
+        pickle.dump(dict(cases=cases), fh, protocol=4)
+    print(f"hybrid_inputs_golden.pkl: {len(cases)} segments, "
+          f"{sum(c['bonus'] is not None for c in cases)} with a bonus")
 
 
 def make_seed(rng):
@@ -900,6 +993,8 @@ if __name__ == "__main__":
         make_extend(np.random.default_rng(303))
     if "hybrid" in which:
         make_hybrid(np.random.default_rng(404))
+    if "hybrid_inputs" in which:
+        make_hybrid_inputs(np.random.default_rng(909))
     if "seed" in which:
         make_seed(np.random.default_rng(505))
     if "wfa" in which:

@@ -46,8 +46,8 @@ def _select(cands, cfg):
 
 def test_hybrid_inputs_through_the_oracle_match_reference_golden():
     from graphmambaformer_b200.config import ChainingConfig
-    from graphmambaformer_b200.hybrid import (ChainingContext, GraphDistanceOracle, _Sub, graph_bonus,
-                                              sorted_layout, weights)
+    from graphmambaformer_b200.hybrid import (ChainingContext, GraphDistanceOracle, Segment, anchor_weights,
+                                              bonus_rows, sorted_layout)
     from graphmambaformer_b200.types import AnchorSet
 
     with open(os.path.join(GOLDEN, "hybrid_golden.pkl"), "rb") as fh:
@@ -72,9 +72,9 @@ def test_hybrid_inputs_through_the_oracle_match_reference_golden():
             if n == 0:
                 continue
             idx = order[s0: s0 + n]
-            sub = _Sub(a, idx)
-            w = weights(cfg, sub, ctx)
-            b = graph_bonus(cfg, sub, ctx)
+            seg = Segment.of(a, idx)
+            w = anchor_weights(cfg, seg, ctx)
+            b = bonus_rows(cfg, seg, ctx)
             n_bonus += b is not None
             f, parent = oracle.chain_dp(rp[idx] + ln[idx], fp[idx] + ln[idx], w, lut, cfg.max_lookback,
                                         cfg.max_gap, bonus=b)
