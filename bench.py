@@ -315,7 +315,7 @@ def run_b200(args):
     stream = torch.cuda.current_stream(device)
     flush = torch.empty(320 * 1024 * 1024 // 4, dtype=torch.int32, device=device)  # > 126 MB L2
 
-    def sw_leg(name, n_pairs, seed, clocks=None):
+    def sw_leg(name, n_pairs, seed, clocks=None, keep_result=False):
         """Batched and plain device timing plus e2e of one SW workload."""
         ps, params, desc = sw_workload(name, n_pairs, seed=seed)
         sw_p = extension.sw_params(*params)
@@ -340,6 +340,7 @@ def run_b200(args):
         else:
             b_ms = time_device(step("batched"), args.steps, stream, flush)
         barrier()
+        result = extension.fetch(out, dp.n) if keep_result else None  # outputs of the last timed call
         for _ in range(warm):
             step("plain")()
         torch.cuda.synchronize(device)
@@ -419,7 +420,8 @@ def run_b200(args):
         pp = max_over_ranks(pipe) if pipe is not None else None
         return dict(ps=ps, params=params, desc=desc, cells=cells, total=total, batched_ms=b, plain_ms=pl,
                     e2e_ms=c2, sync_ms=c, session_ms=e, pipelined_ms=pp, rank_ms=float(np.mean(b_ms)),
-                    sess_io=sess_io, ctx_io=ctx_io, launches=launches_per_call(dp.max_half_band, True))
+                    sess_io=sess_io, ctx_io=ctx_io, launches=launches_per_call(dp.max_half_band, True),
+                    result=result)
 
     # ---- autotuned scheduling of the batched form (on a 10% sample of the
     # headline workload; outside every timed region) ----
@@ -436,7 +438,8 @@ def run_b200(args):
 
     uuid = str(getattr(torch.cuda.get_device_properties(device), "uuid", ""))
     sampler = ClockSampler(uuid)
-    head = sw_leg(args.workload, args.pairs, 1 + 1000 * rank, clocks=sampler)
+    head = sw_leg(args.workload, args.pairs, 1 + 1000 * rank, clocks=sampler,
+                  keep_result=not args.no_cpu_baseline)
     small = None
     if not args.no_150bp and args.workload != "extension_pairs_150bp":
         small = sw_leg("extension_pairs_150bp", 0, 11 + 1000 * rank)
@@ -597,7 +600,7 @@ def run_b200(args):
         sam_res["roofline"]["peak_source"] = peak_src
         line["sam"] = sam_res
     if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(ps, head["params"])
+        line["cpu_baseline"], line["parity"] = cpu_baseline(ps, head["params"], head["result"])
     return line
 
 
@@ -927,9 +930,10 @@ def stratified_sample(ps, max_cells: float, seed: int = 0) -> np.ndarray:
     return np.sort(np.concatenate(picks))
 
 
-def oracle_sw_rate(ps, params, idx, threads):
+def oracle_sw_rate(ps, params, idx, threads, want_out=False):
     """GCUPS of the C oracle (the reference algorithm, SW + traceback) on the
-    pairs ``idx`` of ``ps``; returns (gcups, cells, seconds)."""
+    pairs ``idx`` of ``ps``; returns (gcups, cells, seconds), plus the
+    oracle's outputs when ``want_out``."""
     from graphmambaformer_b200.synth import band_cells
     from oracle import oracle
 
@@ -937,18 +941,41 @@ def oracle_sw_rate(ps, params, idx, threads):
     ts = [ps.t(int(b)) for b in idx]
     cs = float(band_cells(ps.query_len[idx], ps.target_len[idx], ps.half_band[idx], ps.band_offset[idx]).sum())
     t0 = time.perf_counter()
-    oracle.sw_batch(qs, ts, ps.half_band[idx], ps.band_offset[idx], *params, threads=threads)
+    res = oracle.sw_batch(qs, ts, ps.half_band[idx], ps.band_offset[idx], *params, threads=threads)
     dt = time.perf_counter() - t0
-    return cs / dt / 1e9, cs, dt
+    return (cs / dt / 1e9, cs, dt, res) if want_out else (cs / dt / 1e9, cs, dt)
 
 
-def cpu_baseline(ps, params, max_cells: float = 6e9) -> dict:
+def sw_mismatches(got, want, idx) -> int:
+    """Pairs of ``idx`` whose GPU result (``got``, indexed by pair) differs
+    from the oracle's (``want``, indexed by sample position) in any field:
+    score, ends, starts, op counts or CIGAR."""
+    bad = 0
+    for k, b in enumerate(idx):
+        b = int(b)
+        same = (np.float32(got.score[b]) == want.score[k] and got.query_end[b] == want.query_end[k]
+                and got.target_end[b] == want.target_end[k] and got.query_start[b] == want.query_start[k]
+                and got.target_start[b] == want.target_start[k]
+                and np.array_equal(got.op_counts[b], want.counts[k]) and got.cigar(b) == want.cigars[k])
+        bad += 0 if same else 1
+    return bad
+
+
+def cpu_baseline(ps, params, got=None, max_cells: float = 6e9):
+    """The oracle timed on a stratified sample of the workload; its outputs
+    are compared with the GPU's outputs ``got`` of the same pairs.  Returns
+    (cpu_baseline dict, parity dict or None)."""
     th = host_threads()
     idx = stratified_sample(ps, max_cells)
-    gcups, cs, dt = oracle_sw_rate(ps, params, idx, th)
-    return {"value": gcups, "unit": "GCUPS", "cores": th, "kind": "port",
+    gcups, cs, dt, want = oracle_sw_rate(ps, params, idx, th, want_out=True)
+    base = {"value": gcups, "unit": "GCUPS", "cores": th, "kind": "port",
             "sample": f"{len(idx)} pairs ({cs:.3g} cells, every length decile) of the same workload, "
                       f"SW + traceback, C restatement of the reference, {dt:.1f} s"}
+    parity = None
+    if got is not None:
+        parity = {"pairs": int(len(idx)), "mismatches": sw_mismatches(got, want, idx),
+                  "fields": "score, ends, starts, op counts, CIGAR of the last timed call vs the oracle"}
+    return base, parity
 
 
 def run_reference(args):
@@ -1025,6 +1052,55 @@ def profile_case(args):
     print(json.dumps({"profile_case": "done", "cells_per_launch": ps.cells()}))
 
 
+def _r(x, nd=4):
+    """A figure rounded to ``nd`` significant digits (None stays None)."""
+    if x is None:
+        return None
+    return float(f"{float(x):.{nd}g}")
+
+
+def compact_summary(line: dict) -> dict:
+    """The figures of every leg in a few hundred bytes.  It goes last on the
+    line, so that a reader keeping only the end of a long line still sees
+    them."""
+    s = {"headline_gcups": _r(line.get("value")), "e2e_gcups": _r(line.get("e2e", {}).get("value")),
+         "int_frac": _r(line.get("roofline", {}).get("frac"), 3)}
+    pl = line.get("plain")
+    if pl:
+        s["plain_gcups"] = _r(pl["value"])
+        s["batched_over_plain"] = _r(pl["batched_over_plain"], 3)
+    sm = line.get("extension_150bp")
+    if sm:
+        s["bp150"] = {"gcups": _r(sm["value"]), "plain": _r(sm["plain"]), "e2e": _r(sm["e2e"]["value"])}
+    ch = line.get("chain")
+    if ch:
+        s["chain"] = {"anchors_s": _r(ch["value"]), "ms": _r(ch["ms_per_step"]), "e2e_anchors_s": _r(ch["e2e"]["value"]),
+                      "f64_frac": _r(ch.get("roofline", {}).get("frac"), 3)}
+    sv = line.get("serving")
+    if sv:
+        s["serving"] = [{"offered": int(p["offered_reads_per_s"]), "achieved": _r(p["achieved_reads_per_s"]),
+                         "p50_ms": _r(p["p50_ms"], 3), "p99_ms": _r(p["p99_ms"], 3)} for p in sv["loads"]]
+    lr = line.get("long_reads")
+    if lr:
+        s["long_reads"] = {"reads": lr["reads"], "chain_anchors_s": _r(lr["chain"]["value"]),
+                           "gap_sw_gcups": _r(lr["gap_sw"]["value"]), "max_half_band": lr["gap_sw"]["max_half_band"]}
+        if "wide_sw" in lr:
+            s["long_reads"]["wide_sw_gcups"] = _r(lr["wide_sw"]["value"])
+            s["long_reads"]["wide_max_half_band"] = lr["wide_sw"]["max_half_band"]
+    wf = line.get("wfa")
+    if wf:
+        s["wfa"] = {"aln_s": _r(wf["value"]), "e2e_aln_s": _r(wf.get("e2e", {}).get("value"))}
+    sa = line.get("sam")
+    if sa:
+        s["sam"] = {"records_s": _r(sa["value"]), "e2e_records_s": _r(sa.get("e2e", {}).get("value"))}
+    if line.get("parity"):
+        s["parity"] = {k: line["parity"][k] for k in ("pairs", "mismatches")}
+    cb = line.get("cpu_baseline")
+    if cb:
+        s["cpu_gcups"] = _r(cb["value"])
+    return s
+
+
 def main():
     args = parse()
     if args.profile_case:
@@ -1032,6 +1108,8 @@ def main():
         return
     line = run_reference(args) if args.impl == "reference" else run_b200(args)
     if line is not None:
+        if args.impl != "reference":
+            line["summary"] = compact_summary(line)
         print(json.dumps(line))
 
 
