@@ -257,6 +257,7 @@ _SIGNATURES = {
                                 POINTER(GmfChainResults), c_void_p, c_size_t, c_void_p]),
     "gmf_chain_batch_noalloc": (c_int, [POINTER(GmfAnchorBatch), POINTER(GmfChainParams), c_void_p,
                                         c_int32, c_int64, POINTER(GmfChainResults), c_void_p]),
+    "gmf_chain_noalloc_error_flags": (c_int, [c_void_p, c_void_p]),
     "gmf_ctx_create": (c_int, [c_int, c_int32, c_size_t, POINTER(c_void_p)]),
     "gmf_ctx_destroy": (c_int, [c_void_p]),
     "gmf_batch_submit": (c_int, [c_void_p, POINTER(GmfHostPairs), POINTER(GmfSwParams), POINTER(GmfHostSwResults),

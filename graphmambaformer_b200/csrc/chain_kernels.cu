@@ -995,7 +995,7 @@ extern "C" int gmf_chain_dp(int32_t n_rows, const int64_t* row_off, const int32_
     if (n_rows == 0) return GMF_OK;
     if (!row_off || !read_end || !ref_end || !weight || !f || !parent) return GMF_ERR_INVALID_ARGUMENT;
     if (!valid_lut(pen_lut, lut_len, max_gap)) return GMF_ERR_INVALID_ARGUMENT;
-    GMF_TRY(bind_stream_device((cudaStream_t)stream));
+    GMF_BIND_STREAM(stream);
     DpArgs d{};
     d.row_off = row_off;
     d.read_end = read_end;
@@ -1019,7 +1019,7 @@ extern "C" int gmf_chain_sort(const gmf_anchor_batch* an, const gmf_sorted_ancho
         !so->perm || !so->n_plus || !so->n_minus || !so->read_end || !so->ref_end)
         return GMF_ERR_INVALID_ARGUMENT;
     if (!workspace || workspace_bytes < 256) return GMF_ERR_WORKSPACE;
-    GMF_TRY(bind_stream_device((cudaStream_t)stream));
+    GMF_BIND_STREAM(stream);
     // reads too large for shared memory sort in 12 * 2 bytes per anchor of
     // workspace (gmf_chain_workspace_bytes covers it)
     const size_t A = (workspace_bytes - 256) / 24;
@@ -1071,7 +1071,7 @@ extern "C" int gmf_chain_batch(const gmf_anchor_batch* an, const gmf_chain_param
     if (!valid_lut(pen_lut, lut_len, cp->max_gap)) return GMF_ERR_INVALID_ARGUMENT;
     if ((sorted_weight || sorted_bonus) && !sorted_in) return GMF_ERR_INVALID_ARGUMENT;
     if (!workspace) return GMF_ERR_WORKSPACE;
-    GMF_TRY(bind_stream_device(stream));
+    GMF_BIND_STREAM(stream);
 
     // the host does not know n_anchors (device CSR); the caller sized the
     // workspace with gmf_chain_workspace_bytes, so derive A from its size.
@@ -1225,11 +1225,20 @@ extern "C" int gmf_chain_batch_noalloc(const gmf_anchor_batch* an, const gmf_cha
     const size_t need = gmf_chain_workspace_bytes(an->n_reads, n_anchors);
     if (need > GMF_CHAIN_NOALLOC_SCRATCH_BYTES) return GMF_ERR_LIMIT;
     if (an->n_reads == 0) return GMF_OK;
-    GMF_TRY(bind_stream_device((cudaStream_t)stream));
+    GMF_BIND_STREAM(stream);
     void* scratch = nullptr;
     GMF_TRY(chain_scratch_address(&scratch));
     // gmf_chain_batch clears the error word itself; every other scratch array
     // is written before it is read (sort keys, DP values, claimed flags)
     return gmf_chain_batch(an, cp, pen_lut, lut_len, nullptr, nullptr, nullptr, res, scratch, need,
                            stream);
+}
+
+extern "C" int gmf_chain_noalloc_error_flags(int32_t* flags, gmf_stream_t stream) {
+    if (!flags) return GMF_ERR_INVALID_ARGUMENT;
+    GMF_BIND_STREAM(stream);
+    void* scratch = nullptr;
+    GMF_TRY(chain_scratch_address(&scratch));
+    // the error word is the first word of the scratch (gmf_chain_batch's layout)
+    return cuda_status(cudaMemcpyAsync(flags, scratch, sizeof(int32_t), cudaMemcpyDefault, (cudaStream_t)stream));
 }

@@ -40,7 +40,7 @@ extern "C" int gmf_gather_segments(const int8_t* src, int64_t src_len, int32_t n
     if (n < 0 || src_len < 0) return GMF_ERR_INVALID_ARGUMENT;
     if (n == 0) return GMF_OK;
     if (!src || !start || !len || !dst || !dst_off) return GMF_ERR_INVALID_ARGUMENT;
-    GMF_TRY(gmf::bind_stream_device((cudaStream_t)stream));
+    GMF_BIND_STREAM(stream);
     const int blocks = n < 148 * 16 ? n : 148 * 16;
     gather_segments_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(src, src_len, n, start, len, rc, dst, dst_off);
     return gmf::cuda_status(cudaGetLastError());

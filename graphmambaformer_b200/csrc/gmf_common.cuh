@@ -27,8 +27,10 @@ inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? GMF_OK : GMF_E
 // rather than another runtime's state).  The legacy stream keeps the current
 // device, and so does a stream that is being captured into a CUDA graph:
 // asking a capturing stream for its device invalidates the capture, so a
-// caller that captures selects the device first (gmf_set_device).
-inline int bind_stream_device(cudaStream_t stream) {
+// caller that captures makes the stream's device current first
+// (gmf_set_device).  `prev` receives the device that was current when this
+// call switched it, else stays -1.
+inline int bind_stream_device(cudaStream_t stream, int* prev) {
     if (stream == nullptr) return GMF_OK;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess) return GMF_ERR_CUDA;
@@ -36,9 +38,26 @@ inline int bind_stream_device(cudaStream_t stream) {
     int dev = -1, cur = -1;
     if (cudaStreamGetDevice(stream, &dev) != cudaSuccess) return GMF_ERR_CUDA;
     if (cudaGetDevice(&cur) != cudaSuccess) return GMF_ERR_CUDA;
-    if (dev != cur && cudaSetDevice(dev) != cudaSuccess) return GMF_ERR_CUDA;
+    if (dev != cur) {
+        if (cudaSetDevice(dev) != cudaSuccess) return GMF_ERR_CUDA;
+        *prev = cur;
+    }
     return GMF_OK;
 }
+
+// An entry point's binding to its stream's device: the device that was
+// current before the call is current again when the entry point returns, so
+// no call changes its caller's current device.
+struct StreamDeviceScope {
+    int prev = -1;
+    int status = GMF_OK;
+    explicit StreamDeviceScope(cudaStream_t stream) { status = bind_stream_device(stream, &prev); }
+    ~StreamDeviceScope() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+    StreamDeviceScope(const StreamDeviceScope&) = delete;
+    StreamDeviceScope& operator=(const StreamDeviceScope&) = delete;
+};
 
 }  // namespace gmf
 
@@ -47,6 +66,11 @@ inline int bind_stream_device(cudaStream_t stream) {
         int _s = (expr);           \
         if (_s != GMF_OK) return _s; \
     } while (0)
+
+// Binds the enclosing entry point to the device of `stream` until it returns.
+#define GMF_BIND_STREAM(stream)                                         \
+    gmf::StreamDeviceScope _gmf_device_scope((cudaStream_t)(stream));   \
+    if (_gmf_device_scope.status != GMF_OK) return _gmf_device_scope.status
 
 #define GMF_CUDA_TRY(expr)                          \
     do {                                            \

@@ -340,7 +340,7 @@ extern "C" int gmf_sam_count(const gmf_sam_records* records, int64_t* line_len, 
     GMF_TRY(check(records));
     if (records->n_records == 0) return GMF_OK;
     if (!line_len) return GMF_ERR_INVALID_ARGUMENT;
-    GMF_TRY(gmf::bind_stream_device((cudaStream_t)stream));
+    GMF_BIND_STREAM(stream);
     sam_kernel<false><<<grid_of(records->n_records), SAM_WARPS * 32, 0, (cudaStream_t)stream>>>(
         *records, line_len, nullptr, nullptr, SAM_CHUNK);
     return gmf::cuda_status(cudaGetLastError());
@@ -351,7 +351,7 @@ extern "C" int gmf_sam_fill(const gmf_sam_records* records, const int64_t* line_
     GMF_TRY(check(records));
     if (records->n_records == 0) return GMF_OK;
     if (!line_off || !text) return GMF_ERR_INVALID_ARGUMENT;
-    GMF_TRY(gmf::bind_stream_device((cudaStream_t)stream));
+    GMF_BIND_STREAM(stream);
     // chunks of the longest record's bases (the last chunk takes any remainder)
     const long long mx = records->max_seq_len > 0 ? records->max_seq_len : 0;
     long long ny = (mx + SAM_CHUNK - 1) / SAM_CHUNK;

@@ -232,7 +232,7 @@ extern "C" int gmf_seed_count(const gmf_minimizer_index* idx, int32_t n_reads, c
     if (n_reads < 0) return GMF_ERR_INVALID_ARGUMENT;
     if (n_reads == 0) return GMF_OK;
     if (!codes || !read_off || !counts) return GMF_ERR_INVALID_ARGUMENT;
-    GMF_TRY(gmf::bind_stream_device((cudaStream_t)stream));
+    GMF_BIND_STREAM(stream);
     SeedArgs a = seed_args(idx, n_reads, codes, read_off, both_strands);
     a.counts = (long long*)counts;
     seed_kernel<false><<<seed_grid(n_reads), SEED_THREADS, 0, (cudaStream_t)stream>>>(a);
@@ -248,7 +248,7 @@ extern "C" int gmf_seed_fill(const gmf_minimizer_index* idx, int32_t n_reads, co
     if (n_reads == 0) return GMF_OK;
     if (!codes || !read_off || !anchor_off || !read_pos || !ref_pos || !length || !strand)
         return GMF_ERR_INVALID_ARGUMENT;
-    GMF_TRY(gmf::bind_stream_device((cudaStream_t)stream));
+    GMF_BIND_STREAM(stream);
     SeedArgs a = seed_args(idx, n_reads, codes, read_off, both_strands);
     a.aoff = (const long long*)anchor_off;
     a.read_pos = read_pos;

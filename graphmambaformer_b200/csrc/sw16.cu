@@ -46,6 +46,12 @@
 
 namespace gmf {
 
+// Traceback word of one lane and chunk, byte-planar: bit u (step u of the
+// chunk) of byte h holds "H != diag" of half h, bit 4+u of byte h "F
+// extends"; bit u of byte 2+h holds "H != F", bit 4+u of byte 2+h "E
+// extends".  nib() turns a cell's bits into the walk's 4-bit code (H source
+// 1 diagonal / 2 F / 3 E, F extends, E extends); this form stores no stop
+// bit, the walk stops on the H value it tracks.
 template <int L>
 struct Layout16 {
     const uint32_t* bits;
@@ -56,7 +62,9 @@ struct Layout16 {
         const int v = (i - 1) & (V - 1), s = (i - 1) / V;
         const long long g = (long long)s * P + 2 * v + d;
         const int k = v >> 1, h = v & 1;
-        return (bits[(g >> 2) * L + k] >> (16 * h + 4 * (3 - (int)(g & 3)))) & 15u;
+        const uint32_t w = bits[(g >> 2) * L + k] >> (8 * h + (int)(g & 3));
+        const uint32_t n1 = w & 1u, fc = (w >> 4) & 1u, n2 = (w >> 16) & 1u, ec = (w >> 20) & 1u;
+        return (n1 ? (n2 ? 3u : 2u) : 1u) | (fc << 2) | (ec << 3);
     }
 };
 
@@ -94,19 +102,22 @@ struct Cells16 {
 };
 
 // Scoring constants in packed biased form.
+// (On the scoring divided by its gcd: SwArgs m16, x16, o16, e16.)
 struct K16 {
-    unsigned Z, NEGV, Z2, NEG2, GO2, GE2, MATCH2, NGE2, NZ2, MX;
+    unsigned Z, NEGV, Z2, NEG2, GO2, GE2, MATCH2, NGE2, MX, EB2;
+    int G;  // scale back to the true scores
     __device__ explicit K16(const SwArgs& a) {
+        G = a.g16;
         Z = (unsigned)a.zero16;
         NEGV = (unsigned)a.neg16;
         Z2 = Z * ONE2;
         NEG2 = NEGV * ONE2;
-        GO2 = (unsigned)a.gap_open * ONE2;
-        GE2 = (unsigned)a.gap_extend * ONE2;
-        MATCH2 = (unsigned)a.match * ONE2;
-        NGE2 = ((0x10000u - (unsigned)a.gap_extend) & 0xFFFFu) * ONE2;  // -ext mod 2^16
-        NZ2 = ((0x10000u - Z) & 0xFFFFu) * ONE2;                        // -zero mod 2^16
-        MX = (unsigned)(a.match + a.mismatch);
+        GO2 = (unsigned)a.o16 * ONE2;
+        GE2 = (unsigned)a.e16 * ONE2;
+        MATCH2 = (unsigned)a.m16 * ONE2;
+        NGE2 = ((0x10000u - (unsigned)a.e16) & 0xFFFFu) * ONE2;  // -ext mod 2^16
+        MX = (unsigned)(a.m16 + a.x16);
+        EB2 = (0x8000u - (unsigned)a.e16) * ONE2;  // bit 15 of E_left - E + EB2: E == E_left - ext
     }
     __device__ unsigned init_pk() const { return Z | (NEGV << 16); }  // row 0: H = 0, F = -inf
 };
@@ -183,7 +194,11 @@ __device__ __forceinline__ void row_start16(Cells16& c, int row, int j0, int qle
 // Four pipeline steps of one lane.  The first lane of the group takes its
 // row-above inputs from rv[] when `from_rv` (delay line or previous warp),
 // every other lane from lane k-1 by one shuffle of the packed (H.hi, F.hi).
-template <int L, bool TB, int EM>
+// MASKED: reset out-of-band cells (H = 0, M = E = F = -inf) at every step;
+// the caller drops it for chunks in which every lane of the warp stays
+// inside its band on all four steps (there the reset changes nothing) and
+// advances the band counters itself.
+template <int L, bool TB, int EM, bool MASKED>
 __device__ __forceinline__ void chunk16(Cells16& c, const K16& K, const Grp<L>& grp, int src, unsigned tw,
                                         unsigned tpv, bool from_rv, const unsigned (&rv)[4],
                                         unsigned (&hk)[4], unsigned (&pko)[4]) {
@@ -204,28 +219,34 @@ __device__ __forceinline__ void chunk16(Cells16& c, const K16& K, const Grp<L>& 
         unsigned E = __viaddmax_u16x2(c.el, K.NGE2, ea);
         unsigned H = umax2(M, E);
         if (TB) {
-            const unsigned nz = __viaddmin_u16x2(H, K.NZ2, ONE2);  // H > 0
-            const unsigned n1 = flag2(H - diag);                   // H != diag (H >= diag)
-            const unsigned n2 = flag2(H - F);                      // H != F (H >= F)
-            const unsigned fc = flag2(F - fa);                     // F extends (F >= fa)
-            unsigned ec = 0u;                                      // E extends
-            if (EM == 0) ec = flag2(E - ea);
-            if (EM == 2) ec = flag2(E - (c.el - K.GE2)) ^ ONE2;
-            const unsigned b0 = nz & (~n1 | n2);  // diagonal or E, when H > 0
-            const unsigned b1 = nz & n1;          // F or E
-            const unsigned x = b0 + 2u * b1 + 4u * fc + 8u * ec;
-            c.acc = u == 0 ? x : c.acc * 16u + x;
+            // Each flag is bit 15 of a half of (ordered difference + 0x7fff):
+            // set when the difference is at least 1.  The classifier keeps
+            // every difference within 15 bits, so the sums neither carry nor
+            // borrow across halves.
+            const unsigned n1 = H - diag + 0x7FFF7FFFu;  // H != diag
+            const unsigned n2 = H - F + 0x7FFF7FFFu;     // H != F
+            const unsigned fc = F - fa + 0x7FFF7FFFu;    // F extends (F above - ext > H above - open)
+            unsigned ec = 0u;                            // E extends
+            if (EM == 0) ec = E - ea + 0x7FFF7FFFu;      //   open > ext: E_left - ext > M_left - open
+            if (EM == 2) ec = c.el - E + K.EB2;          //   open < ext: E == E_left - ext (ties extend)
+            // sign-replicated high bytes: [n1.lo n1.hi n2.lo n2.hi], [fc.lo fc.hi ec.lo ec.hi]
+            const unsigned w1 = prmt(n1, n2, 0xFDB9u);
+            const unsigned w2 = prmt(fc, ec, 0xFDB9u);
+            const unsigned b = (w1 & (0x01010101u << u)) | (w2 & (0x10101010u << u));
+            c.acc = u == 0 ? b : (c.acc | b);
         }
-        // in-band mask: slot - lo >= 0 and hi - slot >= 0 per half, kept as
-        // counters biased by 32768 (they never leave [0, 65535], so plain
-        // adds suffice); bit 15 of both set = in band
-        c.ma += ONE2;
-        c.mb -= ONE2;
-        const unsigned m = prmt(c.ma & c.mb, 0u, 0xBB99u);  // 0xFFFF per in-band half
-        H = (H & m) | (K.Z2 & ~m);
-        F = (F & m) | (K.NEG2 & ~m);
-        M = (M & m) | (K.NEG2 & ~m);
-        E = (E & m) | (K.NEG2 & ~m);
+        if (MASKED) {
+            // in-band mask: slot - lo >= 0 and hi - slot >= 0 per half, kept as
+            // counters biased by 32768 (they never leave [0, 65535], so plain
+            // adds suffice); bit 15 of both set = in band
+            c.ma += ONE2;
+            c.mb -= ONE2;
+            const unsigned m = prmt(c.ma & c.mb, 0u, 0xBB99u);  // 0xFFFF per in-band half
+            H = (H & m) | (K.Z2 & ~m);
+            F = (F & m) | (K.NEG2 & ~m);
+            M = (M & m) | (K.NEG2 & ~m);
+            E = (E & m) | (K.NEG2 & ~m);
+        }
         const unsigned pk = prmt(H, F, 0x7632u);  // (H.hi, F.hi)
         unsigned sh = grp.shfl(pk, src);
         if (from_rv) sh = rv[u];
@@ -239,14 +260,35 @@ __device__ __forceinline__ void chunk16(Cells16& c, const K16& K, const Grp<L>& 
     }
 }
 
+// True when every cell of the lane's next chunk (4 steps, both halves) is in
+// band: the first step's lower-bound counters and the last step's upper-
+// bound counters both have bit 15 set.
+__device__ __forceinline__ bool chunk_in_band(const Cells16& c) {
+    return ((c.ma + ONE2) & (c.mb - 4u * ONE2) & 0x80008000u) == 0x80008000u;
+}
+
+// A chunk with or without the band reset: the unmasked form when the whole
+// warp stays in band (warp-uniform decision).
+template <int L, bool TB, int EM>
+__device__ __forceinline__ void chunk16_any(Cells16& c, const K16& K, const Grp<L>& grp, int src, unsigned tw,
+                                            unsigned tpv, bool from_rv, const unsigned (&rv)[4],
+                                            unsigned (&hk)[4], unsigned (&pko)[4]) {
+    if (__all_sync(FULL_MASK, chunk_in_band(c))) {
+        chunk16<L, TB, EM, false>(c, K, grp, src, tw, tpv, from_rv, rv, hk, pko);
+        c.ma += 4u * ONE2;
+        c.mb -= 4u * ONE2;
+    } else {
+        chunk16<L, TB, EM, true>(c, K, grp, src, tw, tpv, from_rv, rv, hk, pko);
+    }
+}
+
 // Best-cell bookkeeping of a chunk: `lb` is the running maximum per half (the
 // row maximum under x-drop); when it grows, the first of the chunk's 4 steps
 // that reaches it gives the position (global step, or slot under x-drop).
 template <bool XD>
 __device__ __forceinline__ void best16(unsigned& lb, int& pos0, int& pos1, const unsigned (&hk)[4], int gstep,
                                        int d) {
-    const unsigned cm = umax2(umax2(hk[0], hk[1]), umax2(hk[2], hk[3]));
-    const unsigned nb = umax2(lb, cm);
+    const unsigned nb = __vimax3_u16x2(lb, __vimax3_u16x2(hk[0], hk[1], hk[2]), hk[3]);
     if (nb != lb) {
         // per half, the steps before the first that reaches nb, counted for
         // both halves at once: nb >= hk[u] in each half, so the plain
@@ -266,10 +308,10 @@ __device__ __forceinline__ void best16(unsigned& lb, int& pos0, int& pos1, const
 // Best cell of a lane (non-x-drop): the first maximum of each half, from its
 // global step, as (score, row, slot).
 template <int L>
-__device__ __forceinline__ void lane_best16(unsigned lb, int pos0, int pos1, unsigned Z, int k, int P,
+__device__ __forceinline__ void lane_best16(unsigned lb, int pos0, int pos1, unsigned Z, int g, int k, int P,
                                             int& bh, int& bi, int& bd) {
     constexpr int V = 2 * L;
-    const int v0 = lo16(lb) - (int)Z, v1 = hi16(lb) - (int)Z;
+    const int v0 = (lo16(lb) - (int)Z) * g, v1 = (hi16(lb) - (int)Z) * g;  // true scores
     int r0 = 0, s0 = 0, r1 = 0, s1 = 0;
     if (v0 > 0) {
         const int tt = pos0 - 2 * (2 * k);
@@ -372,7 +414,7 @@ __device__ void sw16_group(const SwArgs& a, int p, const Grp<L>& grp, uint32_t* 
         }
         const unsigned twin = tw.window();
         unsigned hk[4], pk[4];
-        chunk16<L, TB, EM>(c, K, grp, src, twin, tpv, from_rv, rv, hk, pk);
+        chunk16_any<L, TB, EM>(c, K, grp, src, twin, tpv, from_rv, rv, hk, pk);
         // ---- once per chunk ----
         tpv = prmt(twin, tpv, 0x4344u);  // this chunk's last code, for the next chunk's high half
         tw.advance(active);
@@ -381,8 +423,8 @@ __device__ void sw16_group(const SwArgs& a, int p, const Grp<L>& grp, uint32_t* 
             *reinterpret_cast<uint4*>(ring + (g0 & rmask)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
         best16<XD>(lb, pos0, pos1, hk, g0, d);
         if (XD) {
-            if (d == dW0 && row <= qlen && row >= 1) rowmax[row - 1] = make_int2(lo16(lb) - (int)K.Z, pos0);
-            if (d == dW1 && row + 1 <= qlen && row >= 1) rowmax[row] = make_int2(hi16(lb) - (int)K.Z, pos1);
+            if (d == dW0 && row <= qlen && row >= 1) rowmax[row - 1] = make_int2((lo16(lb) - (int)K.Z) * K.G, pos0);
+            if (d == dW1 && row + 1 <= qlen && row >= 1) rowmax[row] = make_int2((hi16(lb) - (int)K.Z) * K.G, pos1);
         }
         __syncwarp();
         d += 4;
@@ -395,7 +437,7 @@ __device__ void sw16_group(const SwArgs& a, int p, const Grp<L>& grp, uint32_t* 
         if (active && k == 0) record_rowmax(a, p, rowmax);
         xdrop_best<L>(grp, rowmax, qlen, a.x_drop, active, bh, bi, bd);
     } else {
-        lane_best16<L>(lb, pos0, pos1, K.Z, k, P, bh, bi, bd);
+        lane_best16<L>(lb, pos0, pos1, K.Z, K.G, k, P, bh, bi, bd);
 #pragma unroll
         for (int o = L / 2; o > 0; o >>= 1) {
             const int oh = grp.xr(bh, o);
@@ -429,7 +471,7 @@ __device__ void sw16_group(const SwArgs& a, int p, const Grp<L>& grp, uint32_t* 
     rw.init(runs);
     Layout16<L> lay{bits, P, W, qlen};
     int qs = 0, ts = 0;
-    walk<L>(grp, lay, G, qe, te, active && runs_ok && bh > 0, rw, qs, ts);
+    walk<L>(grp, lay, G, a, qe, te, bh, active && runs_ok && bh > 0, rw, qs, ts);
     finish_cigar<L>(a, grp, p, active, rw, runs_ok, qs, ts);
 }
 
@@ -594,7 +636,7 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* pro
             }
             const unsigned twin = tw.window();
             unsigned hk[4], pk[4];
-            chunk16<32, TB, EM>(c, K, grp, src, twin, tpv, lane == 0, rv, hk, pk);
+            chunk16_any<32, TB, EM>(c, K, grp, src, twin, tpv, lane == 0, rv, hk, pk);
             tpv = prmt(twin, tpv, 0x4344u);
             tw.advance(true);
             if (lane == 31) {  // publish before the global store, so the release does not wait on it
@@ -605,8 +647,8 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* pro
             if (TB && kk >= 0 && (g0 >> 2) <= last_chunk) bits[(g0 >> 2) * L + lane] = c.acc;
             best16<XD>(lb, pos0, pos1, hk, g0, d);
             if (XD && kk >= 0) {
-                if (d == dW0 && row <= qlen) rowmax[row - 1] = make_int2(lo16(lb) - (int)K.Z, pos0);
-                if (d == dW1 && row + 1 <= qlen) rowmax[row] = make_int2(hi16(lb) - (int)K.Z, pos1);
+                if (d == dW0 && row <= qlen) rowmax[row - 1] = make_int2((lo16(lb) - (int)K.Z) * K.G, pos0);
+                if (d == dW1 && row + 1 <= qlen) rowmax[row] = make_int2((hi16(lb) - (int)K.Z) * K.G, pos1);
             }
             __syncwarp();
             d += 4;
@@ -617,7 +659,7 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* pro
 
     int bh = 0, bi = 0, bd = 0;
     if (!XD) {
-        lane_best16<L>(lb, pos0, pos1, K.Z, lane, P, bh, bi, bd);
+        lane_best16<L>(lb, pos0, pos1, K.Z, K.G, lane, P, bh, bi, bd);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             const int oh = grp.xr(bh, o);
@@ -670,7 +712,7 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* pro
     rw.init(runs);
     Layout16<L> lay{bits, P, W, qlen};
     int qs = 0, ts = 0;
-    walk<L>(grp, lay, G, qe, te, runs_ok && bh > 0, rw, qs, ts);
+    walk<L>(grp, lay, G, a, qe, te, bh, runs_ok && bh > 0, rw, qs, ts);
     finish_cigar<L>(a, grp, p, true, rw, runs_ok, qs, ts);
 }
 
@@ -746,7 +788,7 @@ __device__ void walk_pair(const SwArgs& a, const Grp<32>& grp, int p, const Pair
     if (!runs_ok && grp.k == 0) atomicOr(a.err, (int)GMF_SWF_WORKSPACE);
     rw.init(runs);
     int qs = 0, ts = 0;
-    walk<32>(grp, lay, G, qe, te, runs_ok && bh > 0, rw, qs, ts);
+    walk<32>(grp, lay, G, a, qe, te, bh, runs_ok && bh > 0, rw, qs, ts);
     finish_cigar<32>(a, grp, p, true, rw, runs_ok, qs, ts);
 }
 

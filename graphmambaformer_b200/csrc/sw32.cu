@@ -200,7 +200,7 @@ __device__ void sw32_pair(const SwArgs& a, int p, const Grp<32>& grp, int2* ring
     rw.init(runs);
     Layout32 lay{bits, P, W, qlen};
     int qs = 0, ts = 0;
-    walk<32>(grp, lay, G, qe, te, runs_ok && bh > 0, rw, qs, ts);
+    walk<32>(grp, lay, G, a, qe, te, bh, runs_ok && bh > 0, rw, qs, ts);
     finish_cigar<32>(a, grp, p, true, rw, runs_ok, qs, ts);
 }
 

@@ -29,17 +29,34 @@ __host__ __device__ inline unsigned long long sw32_tb_words_api(int qlen, int W)
 }
 
 
-// The biased 16x2 form is exact when no 16-bit value can wrap: biased cells
-// lie in [pmax, smax + 4*pmax + 2] with smax = match * (min(qlen, tlen) + 1)
-// and pmax the largest penalty; the traceback compares ordered differences.
+// The biased 16x2 form is exact when no 16-bit value can wrap and no
+// traceback difference leaves 15 bits.  On the gcd-scaled scoring (match m,
+// largest penalty p), biased cells lie in [p, smax + 4p + 2] with smax =
+// m * (min(qlen, tlen) + 1); the step's cells, including those it masks
+// afterwards, stay below smax + 4p + 2 + m, and every difference the
+// traceback flags test (H - diag, H - F, F - (H_up - open), E - (M_left -
+// open), E - (E_left - ext)) is at most smax + 4p + 2 + m.  Flags are bit 15
+// of difference + 0x7fff, exact while that sum stays below 2^16.
 __host__ __device__ inline int max_penalty(int mism, int go, int ge) {
     const int m = mism > go ? mism : go;
     return m > ge ? m : ge;
 }
-__host__ __device__ inline bool fits_int16(int qlen, int tlen, int match, int mism, int go, int ge) {
-    const long long smax = (long long)match * ((qlen < tlen ? qlen : tlen) + 1);
-    const int pmax = max_penalty(mism, go, ge);
-    return pmax <= 2048 && match <= 2048 && smax + 6LL * pmax + 66 <= 65535;
+__host__ __device__ inline int gcd_int(int a, int b) {
+    while (b) {
+        const int t = a % b;
+        a = b;
+        b = t;
+    }
+    return a;
+}
+// g of the scaled scoring: gcd of every parameter that enters a cell value
+__host__ __device__ inline int score_gcd(int match, int mism, int go, int ge) {
+    return gcd_int(gcd_int(match, mism), gcd_int(go, ge));
+}
+__host__ __device__ inline bool fits_int16(int qlen, int tlen, int m16, int x16, int o16, int e16) {
+    const long long smax = (long long)m16 * ((qlen < tlen ? qlen : tlen) + 1);
+    const int p = max_penalty(x16, o16, e16);
+    return p <= 2048 && m16 <= 2048 && smax + 4LL * p + 2 + m16 <= 32768;
 }
 
 // Class of a pair.  Narrow bands share a warp (8 or 16 lanes per pair); wide
@@ -50,7 +67,7 @@ __host__ __device__ inline bool fits_int16(int qlen, int tlen, int match, int mi
 // COOP_PMAX); shorter pairs in those ranges take one warp.
 __host__ __device__ inline int sw_class(int qlen, int tlen, int hb, int match, int mism, int go, int ge,
                                         int l8w, int l16w, const int* cmin) {
-    if (!fits_int16(qlen, tlen, match, mism, go, ge)) return CLS_I32;
+    if (!fits_int16(qlen, tlen, match, mism, go, ge)) return CLS_I32;  // scaled scoring (SwArgs m16...)
     const int W = 2 * hb + 1;
     if (W <= l8w) return CLS_I16_L8;
     if (W <= l16w) return CLS_I16_L16;
@@ -72,7 +89,7 @@ __global__ void sw_classify_kernel(SwArgs a) {
             p = a.order ? a.order[idx] : idx;
             const int ql = (int)(a.q_off[p + 1] - a.q_off[p]);
             const int tl = (int)(a.t_off[p + 1] - a.t_off[p]);
-            cls = sw_class(ql, tl, a.hb[p], a.match, a.mismatch, a.gap_open, a.gap_extend, a.l8w, a.l16w, a.cmin);
+            cls = sw_class(ql, tl, a.hb[p], a.m16, a.x16, a.o16, a.e16, a.l8w, a.l16w, a.cmin);
         }
         const unsigned lt = (1u << lane) - 1u;
 #pragma unroll
@@ -206,7 +223,13 @@ static void fill_args(SwArgs& a, const gmf_pairs* pairs, const gmf_sw_params* pa
     a.cmin[1] = 8;
     a.cmin[2] = 16;
     a.max_hb = pairs->max_half_band;
-    const int pmax = max_penalty(params->mismatch_penalty, params->gap_open, params->gap_extend);
+    const int g = score_gcd(params->match_score, params->mismatch_penalty, params->gap_open, params->gap_extend);
+    a.g16 = g;
+    a.m16 = params->match_score / g;
+    a.x16 = params->mismatch_penalty / g;
+    a.o16 = params->gap_open / g;
+    a.e16 = params->gap_extend / g;
+    const int pmax = max_penalty(a.x16, a.o16, a.e16);
     a.zero16 = 4 * pmax + 2;
     a.neg16 = 2 * pmax;
     a.score = res->score;
@@ -366,7 +389,7 @@ static int sw_prepare(const gmf_pairs* pairs, const gmf_sw_params* params, const
     GMF_TRY(check_common(pairs, params, res));
     const size_t qb = queue_bytes(pairs->n_pairs);
     if (!workspace || workspace_bytes < 256 + qb) return GMF_ERR_WORKSPACE;
-    GMF_TRY(bind_stream_device(stream));
+    GMF_BIND_STREAM(stream);
     GMF_CUDA_TRY(cudaMemsetAsync(workspace, 0, 256 + round_up(2 * N_CLASSES * sizeof(int32_t), 256), stream));
     GMF_CUDA_TRY(cudaMemsetAsync(res->cigar_used, 0, sizeof(unsigned long long), stream));
     GMF_CUDA_TRY(cudaMemsetAsync(res->error_flags, 0, sizeof(int32_t), stream));

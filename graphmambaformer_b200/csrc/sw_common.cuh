@@ -36,6 +36,11 @@ struct SwArgs {
     int32_t max_hb;
     int32_t zero16;                // biased zero of the 16x2 form: 4 * max penalty + 2
     int32_t neg16;                 // biased "-inf" of the 16x2 form: zero16 - (2 * max penalty + 2)
+    // The 16x2 form runs on the scoring divided by g = gcd(match, mismatch,
+    // open, extend): every cell value is a multiple of g, every decision is
+    // a comparison of two cell values, so the scaled DP makes the same
+    // decisions and its scores are the true scores / g.
+    int32_t g16, m16, x16, o16, e16;  // g, and match / mismatch / open / extend divided by g
     int32_t ring;                  // delay-line entries per lane group (power of two)
     unsigned long long* counters;  // [0] workspace words handed out (bump allocator)
     int32_t* queue;                // [N_CLASSES] heads, [N_CLASSES] counts
@@ -309,16 +314,25 @@ __device__ void xdrop_best(const Grp<G>& grp, const int2* rowmax, int qlen, int 
 }
 
 // Warp-cooperative traceback from (qe, te) with the reference's decision
-// order.  `Lay::nib(i, d)` returns the 4-bit cell code (0 outside the band).
+// order.  `Lay::nib(i, d)` returns the 4-bit cell code (0 outside the band):
+// H source (0 stop, 1 diagonal, 2 F, 3 E), "F extends", "E extends".
 // Each iteration the group fetches G cells of its current run -- diagonal
 // (state H), vertical (state F) or horizontal (state E) -- and ballots give
 // the run length and the =/X pattern.  Every lane of the warp executes the
 // same collectives each iteration (groups of one warp may be in different
 // states or already done); only group-uniform scalars depend on the state.
+//
+// The walk also carries the exact score of its current cell, starting from
+// the best score: a diagonal step back subtracts the substitution score, a
+// gap step adds the extension (or, where the gap opens, extension and open)
+// penalty.  The reference stops in state H on a cell whose H is 0; the
+// carried value gives that test, so layouts without a stop code (the 16x2
+// form) stop exactly where the reference does.
 template <int G, class Lay>
-__device__ void walk(const Grp<G>& grp, const Lay& lay, const PairGeo& P, int qe, int te, bool active,
-                     RunWriter& rw, int& i_out, int& j_out) {
+__device__ void walk(const Grp<G>& grp, const Lay& lay, const PairGeo& P, const SwArgs& a, int qe, int te,
+                     int score, bool active, RunWriter& rw, int& i_out, int& j_out) {
     int i = qe, jj = te, state = 0;
+    int v = score;  // H (state 0), F (state 1) or E (state 2) of the current cell
     bool walking = active && i > 0 && jj > 0;
     const int k = grp.k;
     const bool leader = k == 0;
@@ -329,42 +343,61 @@ __device__ void walk(const Grp<G>& grp, const Lay& lay, const PairGeo& P, int qe
         const int dd = state == 0 ? d0 : (state == 1 ? d0 + k : d0 - k);
         const bool valid = walking && ci > 0 && cj > 0;
         const uint32_t nib = valid ? lay.nib(ci, dd) : 0u;
-        const uint32_t cbit = state == 0 ? (((nib & 3u) == 1u) ? 1u : 0u) : (state == 1 ? (nib & 4u) : (nib & 8u));
+        // state H: the substitution score of each lane's cell, and the H value
+        // there (the carried value minus the lanes before it)
+        const bool is_eq = state == 0 && valid && codes_match(P.q[ci - 1], P.t[cj - 1]);
+        const int sub = state == 0 && valid ? (is_eq ? a.match : -a.mismatch) : 0;
+        int incl = sub;
+#pragma unroll
+        for (int o = 1; o < G; o <<= 1) {
+            const int t = grp.up(incl, o);
+            if (k >= o) incl += t;
+        }
+        const int hval = v - (incl - sub);
+        const uint32_t cbit = state == 0 ? (((nib & 3u) == 1u && hval > 0) ? 1u : 0u)
+                                         : (state == 1 ? (nib & 4u) : (nib & 8u));
         const unsigned cont = grp.ballot(valid && cbit);
         const unsigned vm = grp.ballot(valid);
         const int c = lead_ones<G>(cont);
-        const bool mt = state == 0 && valid && k < c && codes_match(P.q[ci - 1], P.t[cj - 1]);
-        const unsigned mm = grp.ballot(mt);
+        const unsigned mm = grp.ballot(is_eq && k < c);
         const int at = c < G ? c : 0;
         const uint32_t nb = grp.shfl(nib, at);
+        const int hv_at = grp.shfl(hval, at);
+        const int total = grp.shfl(incl, G - 1);
         if (walking) {
             if (state == 0) {
                 int pos = 0;
                 while (pos < c) {  // the =/X runs of the c diagonal cells, in walk order
                     const unsigned rest = mm >> pos;
-                    const bool is_eq = rest & 1u;
-                    int len = is_eq ? lead_ones<32>(rest) : (rest ? __ffs(rest) - 1 : 32);
+                    const bool eq = rest & 1u;
+                    int len = eq ? lead_ones<32>(rest) : (rest ? __ffs(rest) - 1 : 32);
                     len = imin(len, c - pos);
-                    rw.add(is_eq ? (int)OP_EQ : (int)OP_X, len, leader);
+                    rw.add(eq ? (int)OP_EQ : (int)OP_X, len, leader);
                     pos += len;
                 }
                 i -= c;
                 jj -= c;
                 if (c < G) {
                     const uint32_t code = nb & 3u;
-                    if (!((vm >> c) & 1u) || code == 0)
+                    if (!((vm >> c) & 1u) || code == 0 || hv_at <= 0) {
                         walking = false;  // off the matrix, or H <= 0: the alignment starts here
-                    else
+                    } else {
                         state = code == 2u ? 1 : 2;
+                        v = hv_at;  // the gap state's value equals H here
+                    }
+                } else {
+                    v -= total;
                 }
             } else {
                 const int gap_op = state == 1 ? (int)OP_I : (int)OP_D;
                 int n;
                 if (c == G) {
                     n = G;
+                    v += G * a.gap_extend;
                 } else if ((vm >> c) & 1u) {
                     n = c + 1;  // the cell that stops extending still emits its gap base
                     state = 0;
+                    v += c * a.gap_extend + a.gap_open;  // H of the cell the gap opened from
                 } else {
                     n = c;      // ran out of rows / columns
                 }

@@ -541,7 +541,7 @@ extern "C" int gmf_wfa_distance(const gmf_wfa_pairs* pairs, int32_t max_distance
     if (pairs->n_pairs == 0) return GMF_OK;
     if (!distance) return GMF_ERR_INVALID_ARGUMENT;
     cudaStream_t st = (cudaStream_t)stream;
-    GMF_TRY(gmf::bind_stream_device(st));
+    GMF_BIND_STREAM(st);
     const int eff = effective(pairs, max_distance);
     const int blocks = grid_blocks(pairs->n_pairs, eff);
     Ws w;
@@ -563,7 +563,7 @@ extern "C" int gmf_wfa_align(const gmf_wfa_pairs* pairs, const int32_t* distance
         !results->cigar_used || !results->error_flags || results->cigar_capacity < 0)
         return GMF_ERR_INVALID_ARGUMENT;
     cudaStream_t st = (cudaStream_t)stream;
-    GMF_TRY(gmf::bind_stream_device(st));
+    GMF_BIND_STREAM(st);
     // the history pass replays each pair to its known distance (<= max_distance)
     const int eff = effective(pairs, max_distance);
     const int blocks = grid_blocks(pairs->n_pairs, eff);

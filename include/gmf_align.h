@@ -14,8 +14,15 @@
  *     other work in the same call (band, x-drop and tie rules are applied per
  *     pair), so a pair aligned alone or inside a large batch gives the same
  *     score, coordinates and CIGAR.
- *   - No call allocates device memory: scratch lives in the caller's
- *     workspace (size it with the *_workspace_bytes helpers).
+ *   - No compute call allocates device memory: scratch lives in the
+ *     caller's workspace (size it with the *_workspace_bytes helpers).  The
+ *     exceptions are gmf_ctx_create and the gmf_batch_* calls, whose
+ *     contexts own their staging and device arenas.
+ *   - A call enqueues on the device that owns its stream and leaves the
+ *     calling thread's current device as it found it.  On a stream that is
+ *     being captured into a CUDA graph the library cannot ask the stream for
+ *     its device, so there the stream's device must be current
+ *     (gmf_set_device) when the call is made.
  *
  * Reference interfaces these entry points replace (GraphMambaFormer):
  *   gmf_banded_sw     graphmambaformer/accel/cuda_kernels.py L504-566 (banded_sw)
@@ -335,7 +342,13 @@ int gmf_chain_batch(const gmf_anchor_batch* anchors, const gmf_chain_params* par
  *              GMF_ERR_LIMIT when gmf_chain_workspace_bytes(n_reads, n_anchors)
  *              exceeds GMF_CHAIN_NOALLOC_SCRATCH_BYTES (about 390,000 anchors).
  *   The first call on a device looks up the array's device address (once per
- *   device, under a lock), so make that first call before any stream capture.
+ *   device, under a lock), so make that first call before any stream capture;
+ *   during a capture the stream's device must be the current device (see the
+ *   conventions above).  The address is kept for the life of the process: a
+ *   cudaDeviceReset between calls is not supported.
+ *   A read with more than GMF_MAX_READ_ANCHORS anchors, or whose anchors lie
+ *   beyond n_anchors (an understated n_anchors), gets zero chains and the
+ *   call still returns GMF_OK; gmf_chain_noalloc_error_flags reports it.
  *   Every call shares the one array per device: calls whose work overlaps on
  *   the GPU (other streams, other threads) race and corrupt each other's
  *   results; serialise them, e.g. on one stream.  The array keeps the last
@@ -343,6 +356,15 @@ int gmf_chain_batch(const gmf_anchor_batch* anchors, const gmf_chain_params* par
 int gmf_chain_batch_noalloc(const gmf_anchor_batch* anchors, const gmf_chain_params* params,
                             const double* pen_lut, int32_t lut_len, int64_t n_anchors,
                             const gmf_chain_results* results, gmf_stream_t stream);
+
+/* Error word of the last gmf_chain_batch_noalloc call on the stream's device,
+ * copied into *flags (device or host memory) on `stream`; with host memory,
+ * read it after the stream has synchronised.  Bits: 1 = a read had more than
+ * GMF_MAX_READ_ANCHORS anchors, 2 = a read's sort did not fit the scratch,
+ * 4 = a read's anchors lay beyond n_anchors; each such read got zero chains.
+ * 0 = every read was chained.  No counterpart in the reference (its chainer
+ * raises on the host instead). */
+int gmf_chain_noalloc_error_flags(int32_t* flags, gmf_stream_t stream);
 
 /* ======================================================================== */
 /* Contexts and asynchronous batches on HOST buffers                        */

@@ -67,7 +67,8 @@ def test_sw_matches_oracle_mixed_profiles(ext):
 
     ps = synth.extension_pairs_mixed(n_pairs=400, seed=7, ref_len=2_000_000, max_len=4000,
                                      log_mean=6.5, log_sigma=0.8)
-    for params in ((2, 4, 4, 2, 0), (2, 4, 6, 2, 600), (1, 3, 5, 1, 40), (3, 2, 2, 2, 25), (2, 5, 1, 3, 0)):
+    for params in ((2, 4, 4, 2, 0), (2, 4, 6, 2, 600), (1, 3, 5, 1, 40), (3, 2, 2, 2, 25), (2, 5, 1, 3, 0),
+                   (3, 6, 9, 3, 0), (4, 6, 10, 2, 301), (6, 6, 6, 6, 0)):
         res = ext.align_pairs(ps, ext.sw_params(*params))
         want = oracle.sw_batch([ps.q(b) for b in range(len(ps))], [ps.t(b) for b in range(len(ps))],
                                ps.half_band, ps.band_offset, *params, threads=8)
@@ -233,22 +234,54 @@ def test_batched_and_plain_forms_agree_on_every_class(ext):
         assert all(a.cigar(k) == b.cigar(k) for k in range(len(ps))), params
 
 
-def test_int16_eligibility_boundary(ext):
-    """Identical sequences whose scores sit just inside and just outside the
-    16-bit range of the batched form (biased cells: score + 6*pmax + 66 <=
-    65535, i.e. up to 32,715 matching bases with these penalties) agree with
-    the plain int32 form and with the closed-form score."""
+@pytest.mark.parametrize("params", [(2, 4, 6, 2, 0), (2, 3, 5, 1, 0)])
+def test_int16_eligibility_boundary(ext, params):
+    """Identical sequences whose lengths sit just inside and just outside the
+    16x2 form's range -- on the scoring divided by g = gcd(match, mismatch,
+    open, extend): m * (len + 1) + 4 * p + 2 + m <= 32768, p the largest
+    scaled penalty (32,752 bases at 2/4/6/2, where g = 2; 16,371 at 2/3/5/1)
+    -- agree with the plain int32 form and with the closed-form score."""
+    from math import gcd
+
     from graphmambaformer_b200 import synth
 
+    g = gcd(gcd(params[0], params[1]), gcd(params[2], params[3]))
+    m, p = params[0] // g, max(params[1], params[2], params[3]) // g
+    last = (32768 - 4 * p - 2 - m) // m - 1
     rng = np.random.default_rng(77)
     qs, ts = [], []
-    for n in (32_700, 32_715, 32_716, 32_800):
+    for n in (last - 1, last, last + 1, last + 40):
         s = synth.random_reference(n, rng)
         qs.append(s)
         ts.append(s.copy())
     ps = synth.PairSet.from_lists(qs, ts, 8, 0)
-    a = ext.align_pairs(ps, ext.sw_params(2, 4, 6, 2, 0), form="batched")
-    b = ext.align_pairs(ps, ext.sw_params(2, 4, 6, 2, 0), form="plain")
-    assert list(a.score) == [2 * len(x) for x in qs]
+    a = ext.align_pairs(ps, ext.sw_params(*params), form="batched")
+    b = ext.align_pairs(ps, ext.sw_params(*params), form="plain")
+    assert list(a.score) == [params[0] * len(x) for x in qs]
     assert np.array_equal(a.score, b.score) and np.array_equal(a.query_end, b.query_end)
     assert all(a.cigar(k) == [("=", len(qs[k]))] for k in range(len(qs)))
+
+
+def test_long_noisy_pairs_near_the_16x2_limit_match_oracle(ext):
+    """ONT-like pairs whose lengths approach the 16x2 range on the scaled
+    scoring (at 2/4/4/2, g = 2: up to 32,756 bases), so traceback
+    differences come close to their 15-bit bound, plus pairs just beyond it
+    (int32 class); bands wide enough for the cooperative classes."""
+    from graphmambaformer_b200 import synth
+    from oracle import oracle
+
+    rng = np.random.default_rng(12)
+    ref = synth.random_reference(200_000, rng)
+    qs, ts, hbs = [], [], []
+    for L, hb in ((32_700, 300), (32_400, 200), (31_000, 600), (33_500, 300)):
+        s = int(rng.integers(1000, 200_000 - L - 1000))
+        qs.append(synth.apply_errors(ref[s: s + L], synth.ONT, rng)[:32_756])
+        ts.append(ref[s: s + L])
+        hbs.append(hb)
+    qs[-1] = ref[5000: 5000 + 33_500].copy()  # identical: its score leaves the 16x2 range
+    ts[-1] = qs[-1].copy()
+    ps = synth.PairSet.from_lists(qs, ts, np.array(hbs, np.int32), 0)
+    for params in ((2, 4, 4, 2, 0), (2, 4, 6, 2, 0)):
+        res = ext.align_pairs(ps, ext.sw_params(*params))
+        want = oracle.sw_batch(qs, ts, ps.half_band, ps.band_offset, *params, threads=4)
+        assert_sw_equal(res, want, label=str(params))

@@ -98,3 +98,41 @@ def test_noalloc_chaining_refuses_batches_beyond_its_scratch():
     assert _noalloc(da, cfg, out) == _native.GMF_OK
     torch.cuda.synchronize()
     assert int(out.n_chains[0].item()) >= 0
+
+
+def test_noalloc_chaining_reports_reads_it_could_not_chain():
+    """An understated n_anchors leaves the later reads outside the scratch's
+    sorted layout: those reads get zero chains, the call still returns
+    GMF_OK, and gmf_chain_noalloc_error_flags reports bit 4.  A correct call
+    afterwards clears the word again."""
+    import torch
+
+    from graphmambaformer_b200 import _native, chaining, synth
+    from graphmambaformer_b200.config import ChainingConfig
+    from graphmambaformer_b200.device import stream_handle
+
+    cfg = ChainingConfig(max_lookback=50, max_gap=5000)
+    b = synth.chaining_reads_hifi(n_reads=6, seed=903, ref_len=2_000_000, mean_len=6_000)
+    a = chaining.AnchorCSR.of(b)
+    da = chaining.upload_anchors(a, "cuda:0")
+    want = chaining.fetch_chains(chaining.launch_chain_batch(da, cfg), a.read_off)
+    assert (want.n_chains > 0).all()
+    flags = torch.full((1,), -1, dtype=torch.int32, device="cuda:0")
+    sp = stream_handle(None, da.device)
+
+    def error_flags():
+        st = _native.lib().gmf_chain_noalloc_error_flags(ctypes.c_void_p(flags.data_ptr()), ctypes.c_void_p(sp))
+        assert st == _native.GMF_OK, _native.status_string(st)
+        return int(flags.item())
+
+    short = chaining.DeviceAnchors(da.n_reads, int(a.read_off[2]), da.read_off, da.read_pos, da.ref_pos,
+                                   da.length, da.strand, da.device)  # room for the first two reads only
+    out = chaining.ChainOutputs.allocate(da, cfg.max_chains)
+    assert _noalloc(short, cfg, out) == _native.GMF_OK
+    got = chaining.fetch_chains(out, a.read_off)
+    assert np.array_equal(got.n_chains[:2], want.n_chains[:2])
+    assert (got.n_chains[2:] == 0).all()
+    assert error_flags() & 4
+    assert _noalloc(da, cfg, out) == _native.GMF_OK
+    _same(chaining.fetch_chains(out, a.read_off), want)
+    assert error_flags() == 0
