@@ -101,27 +101,6 @@ struct Cells16 {
     unsigned acc;                 // traceback nibbles of the chunk
 };
 
-// Scoring constants in packed biased form.
-// (On the scoring divided by its gcd: SwArgs m16, x16, o16, e16.)
-struct K16 {
-    unsigned Z, NEGV, Z2, NEG2, GO2, GE2, MATCH2, NGE2, MX, EB2;
-    int G;  // scale back to the true scores
-    __device__ explicit K16(const SwArgs& a) {
-        G = a.g16;
-        Z = (unsigned)a.zero16;
-        NEGV = (unsigned)a.neg16;
-        Z2 = Z * ONE2;
-        NEG2 = NEGV * ONE2;
-        GO2 = (unsigned)a.o16 * ONE2;
-        GE2 = (unsigned)a.e16 * ONE2;
-        MATCH2 = (unsigned)a.m16 * ONE2;
-        NGE2 = ((0x10000u - (unsigned)a.e16) & 0xFFFFu) * ONE2;  // -ext mod 2^16
-        MX = (unsigned)(a.m16 + a.x16);
-        EB2 = (0x8000u - (unsigned)a.e16) * ONE2;  // bit 15 of E_left - E + EB2: E == E_left - ext
-    }
-    __device__ unsigned init_pk() const { return Z | (NEGV << 16); }  // row 0: H = 0, F = -inf
-};
-
 __device__ __forceinline__ void cells_init(Cells16& c, const K16& K) {
     c.hv = K.Z2;
     c.fv = K.NEG2;
@@ -305,6 +284,43 @@ __device__ __forceinline__ void best16(unsigned& lb, int& pos0, int& pos1, const
     }
 }
 
+// Best-cell bookkeeping without x-drop, branch-free: when a half's running
+// maximum grows, that half's 4 H values of the chunk and the chunk's first
+// global step are kept (a per-half select); the first step that reaches the
+// final maximum is found once, after the DP, from the kept values.  The
+// maximum only grows on a strictly larger value, so the kept chunk is the
+// one in which the final maximum first appears.
+struct BestTrack16 {
+    unsigned sv[4];
+    int g_lo, g_hi;
+    __device__ __forceinline__ void init(unsigned z2) {
+        sv[0] = sv[1] = sv[2] = sv[3] = z2;
+        g_lo = g_hi = 0;
+    }
+    __device__ __forceinline__ void update(unsigned& lb, const unsigned (&hk)[4], int g0) {
+        const unsigned nb = __vimax3_u16x2(lb, __vimax3_u16x2(hk[0], hk[1], hk[2]), hk[3]);
+        // nb >= lb in each half and the difference stays within 15 bits:
+        // bit 15 of difference + 0x7fff is "grew", spread over the half
+        const unsigned up = prmt(nb - lb + 0x7FFF7FFFu, 0u, 0xBB99u);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) sv[u] = (hk[u] & up) | (sv[u] & ~up);
+        g_lo = (up & 1u) ? g0 : g_lo;
+        g_hi = (up >> 31) ? g0 : g_hi;
+        lb = nb;
+    }
+    // Global steps of the first cell of each half that holds its maximum.
+    __device__ __forceinline__ void positions(unsigned lb, int& pos0, int& pos1) const {
+        int u0 = 3, u1 = 3;
+#pragma unroll
+        for (int u = 2; u >= 0; --u) {
+            if (lo16(sv[u]) == lo16(lb)) u0 = u;
+            if (hi16(sv[u]) == hi16(lb)) u1 = u;
+        }
+        pos0 = g_lo + u0;
+        pos1 = g_hi + u1;
+    }
+};
+
 // Best cell of a lane (non-x-drop): the first maximum of each half, from its
 // global step, as (score, row, slot).
 template <int L>
@@ -373,7 +389,7 @@ __device__ void sw16_group(const SwArgs& a, int p, const Grp<L>& grp, uint32_t* 
     const int loop_last = __reduce_max_sync(FULL_MASK, my_last);
     const int last_chunk = my_last >> 2;  // -1 when inactive
 
-    const K16 K(a);
+    const K16& K = a.k16;
     for (int x = k; x < a.ring; x += L) ring[x] = K.init_pk();
     __syncwarp();
     TWin tw;
@@ -388,6 +404,8 @@ __device__ void sw16_group(const SwArgs& a, int p, const Grp<L>& grp, uint32_t* 
     unsigned tpv = 0u;
     unsigned lb = K.Z2;  // best H so far per half (non-x-drop) / row max (x-drop)
     int pos0 = 0, pos1 = 0;
+    BestTrack16 bt;
+    bt.init(K.Z2);
     unsigned rv[4] = {0u, 0u, 0u, 0u};  // delay-line entries of the chunk
     const int src = (k + L - 1) & (L - 1);
     const bool from_rv = use_ring && k == 0;
@@ -421,7 +439,10 @@ __device__ void sw16_group(const SwArgs& a, int p, const Grp<L>& grp, uint32_t* 
         if (TB && (g0 >> 2) <= last_chunk) bits[(g0 >> 2) * L + k] = c.acc;
         if (use_ring && k == L - 1)
             *reinterpret_cast<uint4*>(ring + (g0 & rmask)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-        best16<XD>(lb, pos0, pos1, hk, g0, d);
+        if (XD)
+            best16<XD>(lb, pos0, pos1, hk, g0, d);
+        else
+            bt.update(lb, hk, g0);
         if (XD) {
             if (d == dW0 && row <= qlen && row >= 1) rowmax[row - 1] = make_int2((lo16(lb) - (int)K.Z) * K.G, pos0);
             if (d == dW1 && row + 1 <= qlen && row >= 1) rowmax[row] = make_int2((hi16(lb) - (int)K.Z) * K.G, pos1);
@@ -437,6 +458,7 @@ __device__ void sw16_group(const SwArgs& a, int p, const Grp<L>& grp, uint32_t* 
         if (active && k == 0) record_rowmax(a, p, rowmax);
         xdrop_best<L>(grp, rowmax, qlen, a.x_drop, active, bh, bi, bd);
     } else {
+        bt.positions(lb, pos0, pos1);
         lane_best16<L>(lb, pos0, pos1, K.Z, K.G, k, P, bh, bi, bd);
 #pragma unroll
         for (int o = L / 2; o > 0; o >>= 1) {
@@ -570,7 +592,7 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* pro
     uint32_t* bits = ws;
     int2* rowmax = XD ? reinterpret_cast<int2*>(ws + tbw) : nullptr;
 
-    const K16 K(a);
+    const K16& K = a.k16;
     TWin tw;
     tw.setup(a, G, true);
     const int8_t* __restrict__ q = G.q;
@@ -590,6 +612,8 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* pro
     cells_init(c, K);
     unsigned tpv = 0u, lb = K.Z2;
     int pos0 = 0, pos1 = 0;
+    BestTrack16 bt;
+    bt.init(K.Z2);
     unsigned rv[4] = {INIT, INIT, INIT, INIT};
     const int src = (lane + 31) & 31;
     const int dW0 = (W - 1) & ~3, dW1 = (W + 1) & ~3;
@@ -645,7 +669,10 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* pro
             }
             const int g0 = t + gofs;
             if (TB && kk >= 0 && (g0 >> 2) <= last_chunk) bits[(g0 >> 2) * L + lane] = c.acc;
-            best16<XD>(lb, pos0, pos1, hk, g0, d);
+            if (XD)
+                best16<XD>(lb, pos0, pos1, hk, g0, d);
+            else
+                bt.update(lb, hk, g0);
             if (XD && kk >= 0) {
                 if (d == dW0 && row <= qlen) rowmax[row - 1] = make_int2((lo16(lb) - (int)K.Z) * K.G, pos0);
                 if (d == dW1 && row + 1 <= qlen) rowmax[row] = make_int2((hi16(lb) - (int)K.Z) * K.G, pos1);
@@ -659,6 +686,7 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* pro
 
     int bh = 0, bi = 0, bd = 0;
     if (!XD) {
+        bt.positions(lb, pos0, pos1);
         lane_best16<L>(lb, pos0, pos1, K.Z, K.G, lane, P, bh, bi, bd);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {

@@ -232,6 +232,19 @@ static void fill_args(SwArgs& a, const gmf_pairs* pairs, const gmf_sw_params* pa
     const int pmax = max_penalty(a.x16, a.o16, a.e16);
     a.zero16 = 4 * pmax + 2;
     a.neg16 = 2 * pmax;
+    const unsigned one2 = 0x00010001u;
+    K16& k = a.k16;
+    k.Z = (unsigned)a.zero16;
+    k.NEGV = (unsigned)a.neg16;
+    k.Z2 = k.Z * one2;
+    k.NEG2 = k.NEGV * one2;
+    k.GO2 = (unsigned)a.o16 * one2;
+    k.GE2 = (unsigned)a.e16 * one2;
+    k.MATCH2 = (unsigned)a.m16 * one2;
+    k.NGE2 = ((0x10000u - (unsigned)a.e16) & 0xFFFFu) * one2;
+    k.MX = (unsigned)(a.m16 + a.x16);
+    k.EB2 = (0x8000u - (unsigned)a.e16) * one2;
+    k.G = g;
     a.score = res->score;
     a.q_end = res->query_end;
     a.t_end = res->target_end;

@@ -23,6 +23,19 @@ enum SwClass : int {
     N_CLASSES = 7
 };
 
+// Packed constants of the 16x2 form (each value in both 16-bit halves), on
+// the gcd-scaled scoring; filled on the host so that kernels read them from
+// the parameter bank instead of holding them in registers.
+struct K16 {
+    unsigned Z, NEGV, Z2, NEG2;  // biased zero and "-inf" (plain, packed)
+    unsigned GO2, GE2, MATCH2;   // open, extend, match (packed)
+    unsigned NGE2;               // -extend mod 2^16 (packed)
+    unsigned MX;                 // match + mismatch (a mismatch flag times this is subtracted)
+    unsigned EB2;                // 0x8000 - extend (packed): bit 15 of E_left - E + EB2 is E == E_left - extend
+    int G;                       // gcd of the scoring: true score = scaled score * G
+    __host__ __device__ unsigned init_pk() const { return Z | (NEGV << 16); }  // row 0: H = 0, F = -inf
+};
+
 struct SwArgs {
     const int8_t* q;
     const int64_t* q_off;
@@ -41,6 +54,7 @@ struct SwArgs {
     // a comparison of two cell values, so the scaled DP makes the same
     // decisions and its scores are the true scores / g.
     int32_t g16, m16, x16, o16, e16;  // g, and match / mismatch / open / extend divided by g
+    K16 k16;                          // the 16x2 form's packed constants
     int32_t ring;                  // delay-line entries per lane group (power of two)
     unsigned long long* counters;  // [0] workspace words handed out (bump allocator)
     int32_t* queue;                // [N_CLASSES] heads, [N_CLASSES] counts
