@@ -63,8 +63,10 @@ def parse():
                    help="reads of the long-read stress leg (2,000 = the full configuration; 0 skips it)")
     p.add_argument("--wfa-pairs", type=int, default=20_000, help="pairs of the WFA leg (0: skip it)")
     p.add_argument("--sam-records", type=int, default=25_000, help="records of the SAM leg (0: skip it)")
-    p.add_argument("--serve-loads", default="10000,20000", help="offered loads of the serving leg, reads/s")
-    p.add_argument("--serve-requests", type=int, default=600)
+    p.add_argument("--serve-loads", default="10000,20000,50000,100000,200000",
+                   help="offered loads of the serving leg, reads/s")
+    p.add_argument("--serve-requests", type=int, default=600,
+                   help="requests per load point (at least 1.5 s of arrivals at that load)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile-case", action="store_true",
                    help="small single-GPU case for ncu captures (no timing JSON)")
@@ -340,7 +342,28 @@ def run_b200(args):
         else:
             b_ms = time_device(step("batched"), args.steps, stream, flush)
         barrier()
+        # the same call captured once as a CUDA graph (classifier, class kernels forked onto side streams
+        # and joined, deferred walk) and replayed: one graph launch per step
+        from graphmambaformer_b200 import _native
+
+        _native.check("gmf_set_device", _native.lib().gmf_set_device(device.index))
+        cap = torch.cuda.Stream(device)
+        cap.wait_stream(stream)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=cap, capture_error_mode="thread_local"):
+            extension.launch_banded_sw(dp, sw_p, True, out=out, workspace=ws, stream=cap)
+        stream.wait_stream(cap)
+        for _ in range(warm):
+            graph.replay()
+        torch.cuda.synchronize(device)
+        barrier()
+        g_ms = time_device(graph.replay, args.steps, stream, flush)
+        torch.cuda.synchronize(device)
+        if int(out.error_flags.item()):
+            raise RuntimeError(f"SW kernels reported error flags {int(out.error_flags.item())}")
+        barrier()
         result = extension.fetch(out, dp.n) if keep_result else None  # outputs of the last timed call
+        del graph
         for _ in range(warm):
             step("plain")()
         torch.cuda.synchronize(device)
@@ -413,12 +436,13 @@ def run_b200(args):
         cells = float(desc["cells"])
         total = sum_over_ranks(cells)
         b = max_over_ranks(float(np.mean(b_ms)))
+        gr = max_over_ranks(float(np.mean(g_ms)))
         pl = max_over_ranks(float(np.mean(p_ms)))
         e = max_over_ranks(float(np.mean(e_ms)))
         c = max_over_ranks(float(np.mean(c_ms)))
         c2 = max_over_ranks(c2_ms)
         pp = max_over_ranks(pipe) if pipe is not None else None
-        return dict(ps=ps, params=params, desc=desc, cells=cells, total=total, batched_ms=b, plain_ms=pl,
+        return dict(ps=ps, params=params, desc=desc, cells=cells, total=total, batched_ms=b, graph_ms=gr, plain_ms=pl,
                     e2e_ms=c2, sync_ms=c, session_ms=e, pipelined_ms=pp, rank_ms=float(np.mean(b_ms)),
                     sess_io=sess_io, ctx_io=ctx_io, launches=launches_per_call(dp.max_half_band, True),
                     result=result)
@@ -442,7 +466,22 @@ def run_b200(args):
                   keep_result=not args.no_cpu_baseline)
     small = None
     if not args.no_150bp and args.workload != "extension_pairs_150bp":
+        # its own scheduling knobs, tuned on a 10% sample like the headline's; the headline's are put back
+        # afterwards for the legs that run the mixed workload
+        from graphmambaformer_b200 import autotune
+
+        head_tuning = autotune.get_tuning(device)
+        small_tuning = None
+        if not args.no_autotune:
+            ps_s, params_s, _ = sw_workload("extension_pairs_150bp", 0, seed=11 + 1000 * rank)
+            rng = np.random.default_rng(98)
+            sample = ps_s.subset(np.sort(rng.choice(len(ps_s), size=max(1, len(ps_s) // 10), replace=False)))
+            small_tuning = autotune.autotune_sw(sample, extension.sw_params(*params_s), device, reps=3,
+                                                passes=1).as_dict()
+            del ps_s, sample
         small = sw_leg("extension_pairs_150bp", 0, 11 + 1000 * rank)
+        small["tuning"] = small_tuning or "defaults"
+        autotune.set_tuning(head_tuning, device)
 
     # ---- chaining ----
     chain = None
@@ -550,6 +589,9 @@ def run_b200(args):
                             "ms_per_step": head["session_ms"], "h2d_bytes_per_step": head["sess_io"][0],
                             "d2h_bytes_per_step": head["sess_io"][1],
                             "timing": "wall clock around ExtensionSession.align (Python API)"}},
+        "graph": {"value": head["total"] / (head["graph_ms"] * 1e-3) / 1e9, "unit": "GCUPS",
+                  "ms_per_step": head["graph_ms"],
+                  "form": "the same call captured once as a CUDA graph and replayed (one graph launch per step)"},
         "plain": {"value": plain_gcups, "unit": "GCUPS", "ms_per_step": head["plain_ms"],
                   "form": "gmf_banded_sw_plain: one warp per pair, int32 cells, one launch",
                   "batched_over_plain": gcups / plain_gcups},
@@ -570,6 +612,7 @@ def run_b200(args):
         line["extension_150bp"] = {
             "value": small["total"] / (small["batched_ms"] * 1e-3) / 1e9, "unit": "GCUPS",
             "ms_per_step": small["batched_ms"], "config": small["desc"],
+            "graph": small["total"] / (small["graph_ms"] * 1e-3) / 1e9,
             "plain": small["total"] / (small["plain_ms"] * 1e-3) / 1e9,
             "e2e": {"value": small["total"] / (small["e2e_ms"] * 1e-3) / 1e9, "unit": "GCUPS",
                     "h2d_bytes_per_step": small["ctx_io"][0], "d2h_bytes_per_step": small["ctx_io"][1],
@@ -580,7 +623,7 @@ def run_b200(args):
                                    "unit": "GCUPS", "ms_per_step": small["pipelined_ms"],
                                    "timing": "three batches in flight on a three-slot context"}),
                     "session": small["total"] / (small["session_ms"] * 1e-3) / 1e9},
-            "gpu_launches_per_step": small["launches"]}
+            "gpu_launches_per_step": small["launches"], "tuning": small["tuning"]}
     if chain:
         # about 10 f64/int ops per predecessor evaluation, against this GPU's f64 add/max rate
         ach = CHAIN_OPS_PER_EVAL * chain["pair_evaluations_per_step"] / (chain["ms_per_step"] * 1e-3) / 1e12
@@ -852,12 +895,58 @@ def long_read_leg(args, device, stream, flush, seed: int, warm: int) -> dict:
     torch.cuda.synchronize(device)
     s_ms = float(np.mean(time_device(sstep, args.steps, stream, flush)))
     cells = ps.cells()
+    del out, ws, dp
+    torch.cuda.empty_cache()
+    # wide segmentation: 8 kb segments with half bands up to 2,000; run as calls of <= 5e10 cells each
+    # (0.5 B of traceback bits per cell)
+    segw = al.segments(pool.reads, prim, mode=longreads.WIDE)
+    qw, tw_ = [], []
+    for i in range(len(segw)):
+        read = pool.reads[int(segw.read[i])]
+        frame = read if segw.strand[i] > 0 else synth.reverse_complement(read)
+        qw.append(frame[segw.q_start[i]: segw.q_start[i] + segw.q_len[i]])
+        tw_.append(pool.ref[segw.t_start[i]: segw.t_start[i] + segw.t_len[i]])
+    psw = synth.PairSet.from_lists(qw, tw_, segw.half_band, segw.band_offset)
+    wcells = synth.band_cells(psw.query_len, psw.target_len, psw.half_band, psw.band_offset).astype(np.float64)
+    cut = np.searchsorted(np.cumsum(wcells), np.arange(5e10, wcells.sum() + 5e10, 5e10))
+    bounds = np.unique(np.concatenate([[0], np.minimum(cut + 1, len(psw))]))
+    calls = []
+    for lo, hi in zip(bounds[:-1], bounds[1:]):
+        dpc = extension.upload_pairs(psw.subset(np.arange(lo, hi)), device)
+        calls.append((dpc, extension.SWOutputs.allocate(dpc, True)))
+    wsw = torch.empty(max(extension.workspace_bytes(c[0], True) for c in calls), dtype=torch.uint8, device=device)
+    # the scheduling knobs tuned for these uniform wide pairs on a sample (results checked identical)
+    from graphmambaformer_b200 import autotune
+
+    before = autotune.get_tuning(device)
+    rng = np.random.default_rng(3)
+    sample = psw.subset(np.sort(rng.choice(len(psw), size=min(len(psw), 400), replace=False)))
+    wrep = autotune.autotune_sw(sample, sw_p, device, reps=2, passes=1)
+    del sample
+
+    def wstep():
+        for dpc, outc in calls:
+            extension.launch_banded_sw(dpc, sw_p, True, out=outc, workspace=wsw, stream=stream)
+
+    wstep()
+    torch.cuda.synchronize(device)
+    w_ms = float(np.mean(time_device(wstep, max(1, min(args.steps, 3)), stream, flush)))
+    w_cells = float(wcells.sum())
+    autotune.set_tuning(before, device)
+    wide = {"value": w_cells / (w_ms * 1e-3) / 1e9, "unit": "GCUPS", "ms_per_step": w_ms, "segments": len(segw),
+            "cells": w_cells, "max_half_band": int(segw.half_band.max()),
+            "median_half_band": float(np.median(segw.half_band)), "calls_per_step": len(calls),
+            "tuning": dict(wrep.as_dict(), sample_pairs=400),
+            "segmentation": "primary chain cut at anchors >= 8 kb apart; band clip(32 + |drift| + len/4, 32, 2000)"}
+    del calls, wsw
+    torch.cuda.empty_cache()
     return {"reads": len(pool), "anchors": pool.anchors.n_anchors,
             "chain": {"value": pool.anchors.n_anchors / (c_ms * 1e-3), "unit": "anchors/s", "ms_per_step": c_ms,
                       "lookback": 200},
             "gap_sw": {"value": cells / (s_ms * 1e-3) / 1e9, "unit": "GCUPS", "ms_per_step": s_ms,
                        "segments": len(seg), "cells": cells, "max_half_band": int(seg.half_band.max()),
                        "scoring": "extension defaults 2/4/6/2, x-drop 600"},
+            "wide_sw": wide,
             "config": {"reference": "50 Mb uniform", "reads": "ONT-like 5% error (60% indels), 50-100 kb",
                        "anchors": "raw (k=15, w=10) minimizer hits of the reference's index semantics "
                                   "(max_occ 200), found on the device",
@@ -877,7 +966,7 @@ def serve_leg(args, device, seed: int) -> dict:
 
     pool = synth.mixed_read_pool(n_reads=2000, seed=seed, ref_len=10_000_000)
     index = DeviceMinimizerIndex(pool.ref, k=15, w=10, max_occ=200, device=device)
-    srv = AlignServer(pool.ref, device, budget_bytes=8 << 30, workers=3, max_batch_reads=512, index=index).start()
+    srv = AlignServer(pool.ref, device, budget_bytes=8 << 30, workers=4, max_batch_reads=1024, index=index).start()
     loads = [float(x) for x in str(args.serve_loads).split(",") if x]
     points = []
     try:
@@ -887,7 +976,8 @@ def serve_leg(args, device, seed: int) -> dict:
         for i, load in enumerate(loads):
             srv.completed.clear()
             srv.batches = 0
-            reqs = synth.poisson_requests(args.serve_requests, load, len(pool), seed=seed + 2 + i)
+            n_req = max(args.serve_requests, int(1.5 * load / 32.5))  # 1-64 reads per request, 32.5 on average
+            reqs = synth.poisson_requests(n_req, load, len(pool), seed=seed + 2 + i)
             st = serve_stream(srv, pool, reqs)
             points.append({"offered_reads_per_s": load, "achieved_reads_per_s": st["reads_per_s"],
                            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
@@ -898,7 +988,7 @@ def serve_leg(args, device, seed: int) -> dict:
             "config": {"reference": "10 Mb uniform and its (k=15, w=10) minimizer index, resident on the device",
                        "requests": "1-64 bare reads, Poisson arrivals; seeding, chaining and extension on the GPU",
                        "reads": "pool of 2,000 mixed-profile reads (150 bp - 20 kb)",
-                       "budget": "8 GB", "workers": 3, "max_batch_reads": 512,
+                       "budget": "8 GB", "workers": 4, "max_batch_reads": 1024,
                        "index_bytes": index.bytes}}
 
 
@@ -1063,7 +1153,8 @@ def compact_summary(line: dict) -> dict:
     """The figures of every leg in a few hundred bytes.  It goes last on the
     line, so that a reader keeping only the end of a long line still sees
     them."""
-    s = {"headline_gcups": _r(line.get("value")), "e2e_gcups": _r(line.get("e2e", {}).get("value")),
+    s = {"headline_gcups": _r(line.get("value")), "graph_gcups": _r(line.get("graph", {}).get("value")),
+         "e2e_gcups": _r(line.get("e2e", {}).get("value")),
          "int_frac": _r(line.get("roofline", {}).get("frac"), 3)}
     pl = line.get("plain")
     if pl:
@@ -1071,7 +1162,8 @@ def compact_summary(line: dict) -> dict:
         s["batched_over_plain"] = _r(pl["batched_over_plain"], 3)
     sm = line.get("extension_150bp")
     if sm:
-        s["bp150"] = {"gcups": _r(sm["value"]), "plain": _r(sm["plain"]), "e2e": _r(sm["e2e"]["value"])}
+        s["bp150"] = {"gcups": _r(sm["value"]), "graph": _r(sm.get("graph")), "plain": _r(sm["plain"]),
+                      "e2e": _r(sm["e2e"]["value"])}
     ch = line.get("chain")
     if ch:
         s["chain"] = {"anchors_s": _r(ch["value"]), "ms": _r(ch["ms_per_step"]), "e2e_anchors_s": _r(ch["e2e"]["value"]),

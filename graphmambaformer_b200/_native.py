@@ -241,12 +241,14 @@ _SIGNATURES = {
                                     c_void_p, c_size_t, c_void_p]),
     "gmf_gather_segments": (c_int, [c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_void_p,
                                     c_void_p, c_void_p]),
+    "gmf_chain_spread": (c_int, [POINTER(GmfAnchorBatch), POINTER(GmfChainResults), c_int32, c_void_p, c_void_p]),
     "gmf_seed_count": (c_int, [POINTER(GmfMinimizerIndex), c_int32, c_void_p, c_void_p, c_int32, c_void_p,
                                c_void_p]),
     "gmf_seed_fill": (c_int, [POINTER(GmfMinimizerIndex), c_int32, c_void_p, c_void_p, c_int32, c_void_p,
                               c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "gmf_sw_get_tuning": (c_int, [POINTER(GmfSwTuning)]),
     "gmf_sw_set_tuning": (c_int, [POINTER(GmfSwTuning)]),
+    "gmf_sw_test_coop_wait": (c_int, [c_int32, c_int32]),
     "gmf_chain_dp": (c_int, [c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32,
                              c_int32, c_void_p, c_int32, c_void_p, c_void_p, c_void_p]),
     "gmf_chain_sort": (c_int, [POINTER(GmfAnchorBatch), POINTER(GmfSortedAnchors), c_void_p,

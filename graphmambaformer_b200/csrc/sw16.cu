@@ -541,7 +541,6 @@ __global__ void __launch_bounds__(128) sw16_kernel(SwArgs a) {
 // Traceback words land at the same (global step, lane) positions as in the
 // one-warp layout, so the walk (warp 0, after a block barrier) is unchanged.
 // ---------------------------------------------------------------------------
-constexpr int COOP_WAIT_LIMIT = 1 << 22;  // spins (about 20 ns each) before a wait gives up
 
 // Progress flags between the warps of a CTA: the writer publishes with a
 // release store after its ring store, the reader polls with acquire loads;
@@ -642,7 +641,7 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* pro
                     while (ld_acquire_cta(prog + wprev) < e + 4) {
                         // bounded: after the limit, or once any wait in the grid gave up
                         // (every later wait then ends within ~1k spins), record and go on
-                        if (++spins > COOP_WAIT_LIMIT ||
+                        if (++spins > a.coop_spin_limit ||
                             ((spins & 1023) == 0 && (*(volatile int*)a.err & (int)GMF_SWF_TIMEOUT))) {
                             atomicOr(a.err, (int)GMF_SWF_TIMEOUT);
                             break;
@@ -665,7 +664,7 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* pro
             tw.advance(true);
             if (lane == 31) {  // publish before the global store, so the release does not wait on it
                 *reinterpret_cast<uint4*>(ring_out + (t & rmask)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-                st_release_cta(prog + w, t + 4);
+                if (!a.coop_stall) st_release_cta(prog + w, t + 4);
             }
             const int g0 = t + gofs;
             if (TB && kk >= 0 && (g0 >> 2) <= last_chunk) bits[(g0 >> 2) * L + lane] = c.acc;

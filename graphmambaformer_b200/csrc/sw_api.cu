@@ -15,6 +15,7 @@
 // computes the same integer DP and the same traceback decisions.
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 
 #include "sw_common.cuh"
@@ -116,20 +117,25 @@ static size_t queue_bytes(int n_pairs) {
            round_up((size_t)n_pairs * 8, 256) + round_up((size_t)n_pairs * 4, 256);
 }
 
-// Side streams of the batched form, one per pair class, created once per
-// device.  The class kernels are forked onto them from the caller's stream
-// and joined back before the walk, so a class whose long pairs are draining
-// shares the GPU with the next class instead of idling it.
+// Side streams of the batched form, one per pair class.  The class kernels
+// are forked onto them from the caller's stream and joined back before the
+// walk, so a class whose long pairs are draining shares the GPU with the next
+// class instead of idling it.  Each caller stream gets its own set (created
+// on its first call, up to kSideSets per device; later callers share the
+// last set), so calls from different streams -- the workers of a serving
+// loop -- never queue behind each other on a side stream.
 constexpr int N_SIDE = N_CLASSES;
 struct SideStreams {
+    cudaStream_t owner;  // the caller stream this set serves
     cudaStream_t s[N_SIDE];
     cudaEvent_t fork;
     cudaEvent_t join[N_SIDE];
     bool ready;
 };
 constexpr int kMaxSideDevices = 64;
+constexpr int kSideSets = 16;
 std::mutex g_side_mu;  // guards side streams, tuning, and every fork/launch/join sequence
-SideStreams g_side[kMaxSideDevices];
+SideStreams g_side[kMaxSideDevices][kSideSets];
 
 // Scheduling knobs per device (see gmf_sw_tuning).
 struct Tuning {
@@ -158,17 +164,21 @@ static int current_tuning(gmf_sw_tuning* out) {  // caller holds g_side_mu
     return GMF_OK;
 }
 
-static int side_streams(SideStreams** out) {
+static int side_streams(cudaStream_t owner, SideStreams** out) {  // caller holds g_side_mu
     int dev = 0;
     GMF_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxSideDevices) return GMF_ERR_LIMIT;
-    SideStreams& ss = g_side[dev];
+    SideStreams* sets = g_side[dev];
+    int k = 0;
+    while (k < kSideSets - 1 && sets[k].ready && sets[k].owner != owner) ++k;
+    SideStreams& ss = sets[k];
     if (!ss.ready) {
         for (int i = 0; i < N_SIDE; ++i) {
             GMF_CUDA_TRY(cudaStreamCreateWithFlags(&ss.s[i], cudaStreamNonBlocking));
             GMF_CUDA_TRY(cudaEventCreateWithFlags(&ss.join[i], cudaEventDisableTiming));
         }
         GMF_CUDA_TRY(cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming));
+        ss.owner = owner;
         ss.ready = true;
     }
     *out = &ss;
@@ -202,8 +212,15 @@ static int check_common(const gmf_pairs* pairs, const gmf_sw_params* params, con
     return GMF_OK;
 }
 
+// Test hook of the bounded waits (gmf_sw_test_coop_wait): 0 = the default limit.
+static std::atomic<int> g_test_spin_limit{0};
+static std::atomic<int> g_test_stall{0};
+
 static void fill_args(SwArgs& a, const gmf_pairs* pairs, const gmf_sw_params* params,
                       const gmf_sw_results* res) {
+    const int lim = g_test_spin_limit.load();
+    a.coop_spin_limit = lim > 0 ? lim : COOP_WAIT_LIMIT;
+    a.coop_stall = g_test_stall.load();
     a.q = pairs->query;
     a.q_off = pairs->query_off;
     a.t = pairs->target;
@@ -461,7 +478,7 @@ extern "C" int gmf_banded_sw(const gmf_pairs* pairs, const gmf_sw_params* params
     SideStreams* ss = nullptr;
     const bool fork = tun.side_streams != 0;
     if (fork) {
-        GMF_TRY(side_streams(&ss));
+        GMF_TRY(side_streams(stream, &ss));
         GMF_CUDA_TRY(cudaEventRecord(ss->fork, stream));
     }
     int used = 0;
@@ -565,5 +582,12 @@ extern "C" int gmf_sw_set_tuning(const gmf_sw_tuning* t) {
     std::lock_guard<std::mutex> lock(g_side_mu);
     g_tuning[dev].t = *t;
     g_tuning[dev].set = true;
+    return GMF_OK;
+}
+
+extern "C" int gmf_sw_test_coop_wait(int32_t spin_limit, int32_t stall_writers) {
+    if (spin_limit < 0 || (stall_writers != 0 && stall_writers != 1)) return GMF_ERR_INVALID_ARGUMENT;
+    g_test_spin_limit.store(spin_limit);
+    g_test_stall.store(stall_writers);
     return GMF_OK;
 }

@@ -82,7 +82,13 @@ struct SwArgs {
     int32_t n_xg;
     unsigned long long* rm_base;     // per pair: row maxima (pool offset), ~0 none; null without groups
     int32_t* rm_seen;                // per pair: running row max carried between row chunks
+    int32_t coop_spin_limit;         // polls before a wait between cooperating warps gives up
+    int32_t coop_stall;              // test hook: writers never publish, so every wait runs out
 };
+
+// Polls (each followed by a ~20 ns sleep) before a wait between the warps of
+// a cooperative class gives up and records GMF_SWF_TIMEOUT.
+constexpr int COOP_WAIT_LIMIT = 1 << 22;
 
 // Traceback-bit layout of the int32 form: one 32-bit word per lane per 8
 // steps, 4 bits per step; virtual lane v of strip s handles slot d at step

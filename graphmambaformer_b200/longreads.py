@@ -15,8 +15,14 @@ by both the device path and the oracle parity tests:
 * consecutive kept anchors u, v give one segment: query = read[u.read_pos :
   v.read_pos] (in the chain's orientation), target = ref[u.ref_pos - pad :
   v.ref_pos + pad] clipped to the reference (pad = 32), band offset =
-  u.ref_pos - target start, half band = clip(32 + |drift| + qlen // 50, 32,
-  2000) where drift = (v.ref_pos - u.ref_pos) - (v.read_pos - u.read_pos);
+  u.ref_pos - target start, half band = clip(32 + |drift| + qlen * b //
+  1000, 32, 2000) where drift = (v.ref_pos - u.ref_pos) - (v.read_pos -
+  u.read_pos) and b is the band growth per kb;
+* two modes: ``FINE`` (min_spacing 1,000, b = 20, i.e. qlen // 50: bands of
+  about 50-80 on 1 kb gaps) and ``WIDE`` (min_spacing 8,000, b = 250: the
+  chain cut into 8 kb stretches whose half bands reach the 2,000 limit, the
+  shorter last stretch of each chain below it: the stress configuration's
+  bands up to 2,000);
 * each segment is a local banded SW + traceback with the extension stage's
   scoring (``banded_affine_sw_batch`` + ``traceback_banded`` semantics, B = 1
   per segment), which is what the parity tests compare.
@@ -42,6 +48,11 @@ MIN_SPACING = 1000
 PAD = 32
 BASE_BAND = 32
 MAX_BAND = 2000
+BAND_PER_KB = 20
+
+# segmentation modes: (min_spacing, band growth per kb)
+FINE = (MIN_SPACING, BAND_PER_KB)
+WIDE = (8000, 250)
 
 
 @dataclass
@@ -63,7 +74,7 @@ class Segments:
 
 
 def segment_chain(read_pos: np.ndarray, ref_pos: np.ndarray, ref_len: int,
-                  min_spacing: int = MIN_SPACING, pad: int = PAD):
+                  min_spacing: int = MIN_SPACING, pad: int = PAD, band_per_kb: int = BAND_PER_KB):
     """Segments of one chain from its member anchors (read order): lists of
     (q_start, q_len, t_start, t_len, half_band, band_offset)."""
     rp = np.asarray(read_pos, np.int64)
@@ -84,7 +95,7 @@ def segment_chain(read_pos: np.ndarray, ref_pos: np.ndarray, ref_len: int,
         ts = max(0, int(fp[u]) - pad)
         te = min(ref_len, int(fp[v]) + pad)
         drift = (int(fp[v]) - int(fp[u])) - (qe - qs)
-        hb = int(np.clip(BASE_BAND + abs(drift) + (qe - qs) // 50, BASE_BAND, MAX_BAND))
+        hb = int(np.clip(BASE_BAND + abs(drift) + (qe - qs) * band_per_kb // 1000, BASE_BAND, MAX_BAND))
         out.append((qs, qe - qs, ts, max(te - ts, 0), hb, int(fp[u]) - ts))
     return out
 
@@ -120,13 +131,16 @@ class LongReadAligner(BatchAligner):
             out.append((int(ch[0].strand), a.read_pos[g][order], a.ref_pos[g][order]))
         return out, res
 
-    def segments(self, reads, primaries) -> Segments:
+    def segments(self, reads, primaries, mode=FINE) -> Segments:
+        """Gap segments of the primary chains under a segmentation mode
+        (``FINE`` or ``WIDE``)."""
         cols = [[] for _ in range(8)]
+        spacing, per_kb = mode
         for r, pc in enumerate(primaries):
             if pc is None:
                 continue
             strand, rp, fp = pc
-            for s in segment_chain(rp, fp, self.ref_len):
+            for s in segment_chain(rp, fp, self.ref_len, min_spacing=spacing, band_per_kb=per_kb):
                 for c, v in zip(cols, (r, strand) + s):
                     c.append(v)
         return Segments(np.array(cols[0], np.int64), np.array(cols[1], np.int8), np.array(cols[2], np.int64),

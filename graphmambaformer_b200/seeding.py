@@ -47,7 +47,8 @@ class DeviceMinimizerIndex:
                     stream: Optional[torch.cuda.Stream] = None) -> dict:
         """Seed reads already on the device (codes CSR).  Returns device
         tensors read_off (n_reads + 1, per read: forward then reverse
-        anchors), read_pos, ref_pos, length, strand and the anchor count."""
+        anchors), read_pos, ref_pos, length, strand, the anchor count and the
+        largest read's anchor count."""
         s = stream or torch.cuda.current_stream(self.device)
         sp = int(s.cuda_stream)
         bind(self.device, sp)
@@ -64,7 +65,10 @@ class DeviceMinimizerIndex:
             aoff = torch.zeros(2 * n_reads + 1, dtype=torch.int64, device=self.device)
             if n_reads:
                 torch.cumsum(counts[: 2 * n_reads], 0, out=aoff[1:])
-            total = int(aoff[-1].item())  # sizes the outputs (one host round trip)
+            # the total sizes the outputs; the largest read is checked against the chaining limit (one
+            # host round trip for both)
+            per_read = (counts[0: 2 * n_reads: 2] + counts[1: 2 * n_reads: 2]).max() if n_reads else counts[0] * 0
+            total, most = (int(x) for x in torch.stack([aoff[-1], per_read]).cpu().tolist())
             i32 = dict(dtype=torch.int32, device=self.device)
             out = dict(read_pos=torch.empty(max(total, 1), **i32), ref_pos=torch.empty(max(total, 1), **i32),
                        length=torch.empty(max(total, 1), **i32),
@@ -75,6 +79,7 @@ class DeviceMinimizerIndex:
                 vp(out["ref_pos"].data_ptr()), vp(out["length"].data_ptr()), vp(out["strand"].data_ptr()), vp(sp)))
             out["read_off"] = aoff[::2].contiguous()
         out["n_anchors"] = total
+        out["max_read_anchors"] = most
         return out
 
     def seed(self, reads: Sequence[np.ndarray], both_strands: bool = True) -> AnchorCSR:

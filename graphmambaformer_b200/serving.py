@@ -42,9 +42,8 @@ from . import _native
 from .chaining import LUTS, AnchorCSR, ChainingConfig, chain_params
 from .config import ExtensionConfig
 from .device import bind, require_cuda
-from .extension import SWResult, _result, longest_first, params_from_config
+from .extension import longest_first, params_from_config
 from .session import _Buffers
-from .types import add_soft_clips
 
 
 def estimate_bytes(read_lens: np.ndarray, n_anchors: int, cfg: ExtensionConfig, max_chains: int) -> int:
@@ -53,6 +52,67 @@ def estimate_bytes(read_lens: np.ndarray, n_anchors: int, cfg: ExtensionConfig, 
     W = 2 * cfg.max_half_band + 1
     cells = int(np.sum((np.asarray(read_lens, np.int64) + 2 * cfg.flank) * W)) * min(max_chains, 2)
     return int(120 * n_anchors + cells // 2 + 64 * len(read_lens) + (1 << 20))
+
+
+class BatchAlignments:
+    """The alignments of a batch of reads, kept as arrays: one entry per kept
+    chain, chains in read order and, within a read, in select order.  Item
+    ``i`` is read i's list of ExtensionResults (as AffineChainer.chain +
+    ExtensionEngine.extend_chains give them), built when it is read; a slice
+    is a view of a range of reads.  Holding the batch as arrays keeps the
+    serving loop free of per-chain Python work; a client pays for the
+    objects of the reads it looks at."""
+
+    def __init__(self, n_reads: int, chain_off: np.ndarray, cols: Optional[dict] = None,
+                 words: Optional[np.ndarray] = None, objects: Optional[list] = None, lo: int = 0,
+                 hi: Optional[int] = None):
+        self.n_reads = int(n_reads)
+        self.chain_off = chain_off  # n_reads + 1: the chains of read r are chain_off[r] .. chain_off[r+1]-1
+        self.cols = cols            # per chain: score, qs, qe, ts, te, counts (C, 4), cstart, clen, clip_l, clip_r
+        self.words = words          # CIGAR words (run << 4 | op), without the soft clips
+        self.objects = objects      # or per chain, ready ExtensionResults (the WFA path)
+        self.lo = int(lo)
+        self.hi = self.n_reads if hi is None else int(hi)
+
+    @staticmethod
+    def empty(n_reads: int) -> "BatchAlignments":
+        return BatchAlignments(n_reads, np.zeros(n_reads + 1, np.int64), objects=[])
+
+    def __len__(self) -> int:
+        return self.hi - self.lo
+
+    def _chain(self, c: int):
+        from .types import ExtensionResult, add_soft_clips, words_to_cigar
+
+        if self.objects is not None:
+            return self.objects[c]
+        k = self.cols
+        s0, n = int(k["cstart"][c]), int(k["clen"][c])
+        cnt = k["counts"][c]
+        return ExtensionResult(
+            score=float(k["score"][c]),
+            cigar=add_soft_clips(words_to_cigar(self.words[s0: s0 + n]), int(k["clip_l"][c]), int(k["clip_r"][c])),
+            read_start=int(k["qs"][c]), read_end=int(k["qe"][c]), ref_start=int(k["ts"][c]),
+            ref_end=int(k["te"][c]), n_match=int(cnt[0]), n_mismatch=int(cnt[1]), n_insertion=int(cnt[2]),
+            n_deletion=int(cnt[3]))
+
+    def __getitem__(self, i):
+        if isinstance(i, slice):
+            a, b, step = i.indices(len(self))
+            if step != 1:
+                raise ValueError("BatchAlignments slices take consecutive reads")
+            return BatchAlignments(self.n_reads, self.chain_off, self.cols, self.words, self.objects,
+                                   self.lo + a, self.lo + max(a, b))
+        if i < 0:
+            i += len(self)
+        if not 0 <= i < len(self):
+            raise IndexError(i)
+        r = self.lo + i
+        return [self._chain(c) for c in range(int(self.chain_off[r]), int(self.chain_off[r + 1]))]
+
+    def __iter__(self):
+        for i in range(len(self)):
+            yield self[i]
 
 
 class BatchAligner:
@@ -99,20 +159,19 @@ class BatchAligner:
             sd = self.index.seed_device(reads_d, up("roff", roff, s), R, True, stream=s)
             ro, rp, fp, ln, st = sd["read_off"], sd["read_pos"], sd["ref_pos"], sd["length"], sd["strand"]
             A = int(sd["n_anchors"])
-            with torch.cuda.stream(s):  # host copies for the window spans, after the fill on this stream
-                a = AnchorCSR(ro.cpu().numpy(), rp[:A].cpu().numpy(), fp[:A].cpu().numpy(), ln[:A].cpu().numpy(),
-                              st[:A].cpu().numpy())
+            per_read = int(sd["max_read_anchors"])
         else:
             a = AnchorCSR.of(anchors)
             if R != len(a):
                 raise ValueError("one anchor set per read is required")
             A = int(a.read_off[-1])
+            per_read = int(np.diff(a.read_off).max(initial=0))
             ro = up("ro", a.read_off, s)
             rp = up("rp", pad(a.read_pos, np.int32), s)
             fp = up("fp", pad(a.ref_pos, np.int32), s)
             ln = up("ln", pad(a.length, np.int32), s)
             st = up("st", pad(a.strand, np.int8), s)
-        if np.diff(a.read_off).max(initial=0) > _native.MAX_READ_ANCHORS:
+        if per_read > _native.MAX_READ_ANCHORS:
             raise ValueError(f"a read has more than {_native.MAX_READ_ANCHORS} anchors")
         mc = self.cp.max_chains
         o = dict(n=db("n", R, torch.int32), score=db("score", R * mc, torch.float64),
@@ -128,44 +187,34 @@ class BatchAligner:
         self._call("gmf_chain_batch", ctypes.byref(batch_c), ctypes.byref(self.cp),
                    ctypes.c_void_p(self.lut.data_ptr()), self.lut.numel(), None, None, None, ctypes.byref(res_c),
                    ctypes.c_void_p(ws.data_ptr()), need, ctypes.c_void_p(sp))
+        # the diagonal spread of every chain, on the device beside the chain records
+        spread_d = db("spread", R * mc, torch.int32)
+        self._call("gmf_chain_spread", ctypes.byref(batch_c), ctypes.byref(res_c), mc,
+                   ctypes.c_void_p(spread_d.data_ptr()), ctypes.c_void_p(sp))
         dl = self.buf.download
-        h = {k: dl("h_" + k, o[k], n, s) for k, n in
-             (("n", R), ("strand", R * mc), ("span", 4 * R * mc), ("nmem", R * mc), ("mem", A))}
+        h = {k: dl("h_" + k, t, n, s) for k, t, n in
+             (("n", o["n"], R), ("strand", o["strand"], R * mc), ("span", o["span"], 4 * R * mc),
+              ("spread", spread_d, R * mc))}
         s.synchronize()
-        n_ch = h["n"][:R].numpy()
+        n_ch = np.minimum(h["n"][:R].numpy(), mc)
         strand = h["strand"][: R * mc].numpy().reshape(R, mc)
         span = h["span"][: 4 * R * mc].numpy().reshape(R, mc, 4)
-        nmem = h["nmem"][: R * mc].numpy().reshape(R, mc)
-        mem = h["mem"][:A].numpy()
+        spread_all = h["spread"][: R * mc].numpy().reshape(R, mc)
 
         # ---- one pair per kept chain, in read order ----
         cr, ck = np.nonzero(np.arange(mc)[None, :] < n_ch[:, None])  # (read, slot) of every chain
         C = len(cr)
-        results: list = [[] for _ in range(R)]
+        chain_off = np.zeros(R + 1, np.int64)
+        np.cumsum(n_ch, out=chain_off[1:])
         if C == 0:
-            return results
-        m = nmem[cr, ck].astype(np.int64)
-        # members of chain (r, k) start after the members of slots < k of read r
-        first = a.read_off[cr] + (np.cumsum(nmem, axis=1) - nmem)[cr, ck]
-        seg = np.zeros(C + 1, np.int64)
-        np.cumsum(m, out=seg[1:])
-        flat = np.repeat(first - seg[:-1], m) + np.arange(int(seg[-1]), dtype=np.int64)
-        gidx = a.read_off[np.repeat(cr, m)] + mem[flat]
-        dg = a.ref_pos[gidx].astype(np.int64) - a.read_pos[gidx].astype(np.int64)
-        nz = m > 0
-        spread = np.zeros(C, np.int64)
-        if nz.any():
-            starts = seg[:-1][nz]
-            spread[nz] = np.maximum.reduceat(dg, starts) - np.minimum.reduceat(dg, starts)
+            return BatchAlignments.empty(R)
+        spread = spread_all[cr, ck].astype(np.int64)
         rc = strand[cr, ck] < 0
         sp4 = span[cr, ck].astype(np.int64)  # read_start, read_end, ref_start, ref_end
         if self.ecfg.algorithm == "wfa":
-            ext = self._extend_wfa(R, rl, roff, reads_d, cr, rc, sp4, spread)
-        else:
-            ext = self._extend_sw(R, rl, roff, reads_d, cr, rc, sp4, spread, shared=True)
-        for c in range(C):
-            results[int(cr[c])].append(ext[c])
-        return results
+            return BatchAlignments(R, chain_off, objects=self._extend_wfa(R, rl, roff, reads_d, cr, rc, sp4, spread))
+        cols, words = self._extend_sw(R, rl, roff, reads_d, cr, rc, sp4, spread, shared=True)
+        return BatchAlignments(R, chain_off, cols, words)
 
     def _gather(self, tag: str, reads_d, roff, rl, cr, rc, wstart, wlen) -> tuple:
         """Queries (reverse-complemented for strand -1) and reference
@@ -247,20 +296,22 @@ class BatchAligner:
         used = int(hh["used"][0])
         words = dl("h2_cigar", cigar, used, s)
         s.synchronize()
-        res = SWResult(hh["score"][:C].numpy(), hh["qe"][:C].numpy(), hh["te"][:C].numpy(),
-                       hh["qs"][:C].numpy(), hh["ts"][:C].numpy(), hh["counts"][: 4 * C].numpy().reshape(C, 4),
-                       words[:used].numpy().view(np.uint32), hh["cstart"][:C].numpy(), hh["clen"][:C].numpy(),
-                       int(hh["err"][0]))
-        if res.error_flags:
-            raise RuntimeError(f"gmf_banded_sw reported error flags {res.error_flags}")
-        exts = []
-        for c in range(C):  # ExtensionEngine._finish: window start and soft clips
-            ext = _result(res, c)
-            ext.ref_start += int(wstart[c])
-            ext.ref_end += int(wstart[c])
-            ext.cigar = add_soft_clips(ext.cigar, ext.read_start, int(rlen[c]) - ext.read_end)
-            exts.append(ext)
-        return exts
+        err = int(hh["err"][0])
+        if err:
+            raise RuntimeError(f"gmf_banded_sw reported error flags {err}")
+        # ExtensionEngine._finish as arrays: reference coordinates from the window start, soft clips from
+        # the unaligned ends of the read (copies: the staging buffers are reused by the next batch)
+        qs, qe = hh["qs"][:C].numpy().copy(), hh["qe"][:C].numpy().copy()
+        cols = dict(score=hh["score"][:C].numpy().copy(), qs=qs, qe=qe,
+                    ts=hh["ts"][:C].numpy().astype(np.int64) + wstart,
+                    te=hh["te"][:C].numpy().astype(np.int64) + wstart,
+                    counts=hh["counts"][: 4 * C].numpy().reshape(C, 4).copy(),
+                    cstart=hh["cstart"][:C].numpy().copy(), clen=hh["clen"][:C].numpy().copy(),
+                    clip_l=qs, clip_r=rlen - qe)
+        if not shared:  # the WFA fallback wants ExtensionResults of these chains
+            b = BatchAlignments(C, np.arange(C + 1, dtype=np.int64), cols, words[:used].numpy().view(np.uint32).copy())
+            return [b[c][0] for c in range(C)]
+        return cols, words[:used].numpy().view(np.uint32).copy()
 
     def _extend_wfa(self, R, rl, roff, reads_d, cr, rc, sp4, spread) -> list:
         """The extension's wfa mode (extension.py L643-730) on the gathered
@@ -470,8 +521,11 @@ def _serve_stream(server: AlignServer, pool, requests: list, time_scale: float =
         wait = t0 + arr * time_scale - time.perf_counter()
         if wait > 0:
             time.sleep(wait)
-        reads, anchors = pool.take(idx)
-        futs.append(server.submit(reads, None if server.index is not None else anchors))
+        if server.index is not None:  # the server seeds: the request carries bare reads
+            futs.append(server.submit([pool.reads[int(i)] for i in idx]))
+        else:
+            reads, anchors = pool.take(idx)
+            futs.append(server.submit(reads, anchors))
     for f in futs:
         f.result(timeout=600)
     wall = time.perf_counter() - t0

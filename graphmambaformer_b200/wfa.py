@@ -59,24 +59,47 @@ class DeviceWfaPairs:
                                    int(self.h_tlen.sum()), self.max_len)
 
 
-def _csr(seqs: Sequence[np.ndarray]) -> tuple:
-    lens = np.array([len(s) for s in seqs], np.int64)
+# Grow-only pinned staging of the concatenated codes, per (device, side): the
+# sequences are concatenated straight into it, so one host copy and one
+# host-to-device copy move a batch.
+_STAGE: dict = {}
+
+
+def _stage_codes(seqs: Sequence[np.ndarray], side: str, dev: torch.device) -> tuple:
+    """CSR of the sequences on the device: (codes, offsets on the device,
+    host offsets, host lengths).  The copy is enqueued on the current
+    stream; the next call waits for it before it reuses the buffer."""
+    lens = np.fromiter((len(x) for x in seqs), np.int64, len(seqs))
     off = np.zeros(len(seqs) + 1, np.int64)
     np.cumsum(lens, out=off[1:])
-    flat = (np.concatenate([np.asarray(s, np.int8) for s in seqs]) if off[-1] else np.zeros(1, np.int8))
-    return flat, off, lens.astype(np.int32)
+    total = int(off[-1])
+    key = (dev.index, side)
+    h, done = _STAGE.get(key, (None, None))
+    if done is not None:
+        done.synchronize()  # the previous batch's copy out of this buffer has finished
+    if h is None or h.numel() < max(total, 1):
+        h = torch.empty(max(total, 1, int(h.numel() * 1.25) if h is not None else 0), dtype=torch.int8,
+                        pin_memory=True)
+    if total:
+        np.concatenate(seqs, out=h.numpy()[:total], casting="unsafe")
+    d = torch.empty(max(total, 1), dtype=torch.int8, device=dev)
+    done = torch.cuda.Event()
+    if total:
+        d.copy_(h[:total], non_blocking=True)
+    done.record(torch.cuda.current_stream(dev))
+    _STAGE[key] = (h, done)
+    return d, to_device(off, dev), off, lens.astype(np.int32)
 
 
 def upload_wfa_pairs(queries: Sequence[np.ndarray], targets: Sequence[np.ndarray], device=None) -> DeviceWfaPairs:
     if len(queries) != len(targets):
         raise ValueError("queries and targets differ in number")
     dev = require_cuda(device)
-    q, qo, ql = _csr(queries)
-    t, to, tl = _csr(targets)
+    q, qo, _, ql = _stage_codes(queries, "q", dev)
+    t, to, _, tl = _stage_codes(targets, "t", dev)
     if len(queries) and max(ql.max(), tl.max()) > (1 << 28):
         raise ValueError("sequence longer than the library's limit (2^28 codes)")
-    return DeviceWfaPairs(len(queries), to_device(q, dev), to_device(qo, dev), to_device(t, dev), to_device(to, dev),
-                          ql, tl, dev)
+    return DeviceWfaPairs(len(queries), q, qo, t, to, ql, tl, dev)
 
 
 def _check_bound(max_distance: int, max_len: int) -> int:

@@ -237,6 +237,16 @@ int gmf_sw_get_tuning(gmf_sw_tuning* tuning);
  * effect for later gmf_banded_sw calls on that device. */
 int gmf_sw_set_tuning(const gmf_sw_tuning* tuning);
 
+/* Test hook of the cooperative classes' bounded waits (no counterpart in the
+ * reference, whose CPU path has no waits).  A warp of a cooperative class
+ * polls its predecessor's progress flag; after `spin_limit` polls (0 = the
+ * default, about 2^22) it records GMF_SWF_TIMEOUT in the results' error
+ * flags and goes on, so a call never hangs.  With `stall_writers` = 1 no
+ * warp publishes its progress, so every wait runs out: the call returns with
+ * GMF_SWF_TIMEOUT set and meaningless alignments.  Applies to every later
+ * gmf_banded_sw call in the process until reset with (0, 0). */
+int gmf_sw_test_coop_wait(int32_t spin_limit, int32_t stall_writers);
+
 /* ======================================================================== */
 /* Anchor chaining                                                          */
 /* ======================================================================== */
@@ -322,6 +332,14 @@ int gmf_chain_batch(const gmf_anchor_batch* anchors, const gmf_chain_params* par
                     const double* sorted_weight, const double* sorted_bonus,
                     const gmf_chain_results* results, void* workspace, size_t workspace_bytes,
                     gmf_stream_t stream);
+
+/* Diagonal spread of every chain record of gmf_chain_batch: spread[r *
+ * max_chains + k] = max - min of (ref_pos - read_pos) over the member
+ * anchors of read r's slot k (0 for empty slots).  The extension window's
+ * band widening term, computed where the chain records are: replaces the
+ * member loop of alignment/extension.py L489-509 (_window). */
+int gmf_chain_spread(const gmf_anchor_batch* anchors, const gmf_chain_results* chains, int32_t max_chains,
+                     int32_t* spread, gmf_stream_t stream);
 
 /* ======================================================================== */
 /* Chaining without device allocation                                       */

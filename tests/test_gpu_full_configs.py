@@ -8,7 +8,8 @@
 * The HiFi chaining workload: all 5,000 reads of 15 kb +- 20 %, h = 50.
 * The long-read stress workload: 64 ONT-like reads spread over 50-100 kb on
   the 50 Mb reference, chained with h = 200, and every gap segment of each
-  primary chain.
+  primary chain; four of them also with the wide segmentation (8 kb
+  segments, half bands up to 2,000).
 
 The oracle restates ``banded_affine_sw_batch`` + ``traceback_banded``
 (graphmambaformer/alignment/extension.py L78-302) and ``AffineChainer.chain``
@@ -108,3 +109,16 @@ def test_long_read_workload_chains_and_segments_match_oracle():
     exp = oracle.sw_batch(qs, ts, seg.half_band, seg.band_offset, 2, 4, 6, 2, 600, threads=_threads())
     assert len(seg) > 3000
     assert_sw_equal(got, exp, label="long-read gap segments")
+
+    # the wide segmentation (8 kb segments, half bands up to 2,000) on four reads
+    wide = al.segments(pool.reads, prim[:4] + [None] * (len(prim) - 4), mode=longreads.WIDE)
+    assert wide.half_band.max() == longreads.MAX_BAND and wide.half_band.min() < 1500
+    got = al.align_segments(pool.reads, wide)
+    qs, ts = [], []
+    for i in range(len(wide)):
+        read = pool.reads[int(wide.read[i])]
+        frame = read if wide.strand[i] > 0 else synth.reverse_complement(read)
+        qs.append(frame[wide.q_start[i]: wide.q_start[i] + wide.q_len[i]])
+        ts.append(pool.ref[wide.t_start[i]: wide.t_start[i] + wide.t_len[i]])
+    exp = oracle.sw_batch(qs, ts, wide.half_band, wide.band_offset, 2, 4, 6, 2, 600, threads=min(4, _threads()))
+    assert_sw_equal(got, exp, label="long-read wide segments")

@@ -285,3 +285,41 @@ def test_long_noisy_pairs_near_the_16x2_limit_match_oracle(ext):
         res = ext.align_pairs(ps, ext.sw_params(*params))
         want = oracle.sw_batch(qs, ts, ps.half_band, ps.band_offset, *params, threads=4)
         assert_sw_equal(res, want, label=str(params))
+
+
+def test_bounded_cooperative_wait_gives_up_then_recovers(ext):
+    """The waits between the warps of a cooperative class are bounded.  With
+    the test hook making every writer keep its progress to itself, each wait
+    runs out after 256 polls: the call still returns, its error flags carry
+    GMF_SWF_TIMEOUT and the host API raises.  The next normal call on the
+    same device is bit-exact with the oracle again."""
+    import torch
+
+    from graphmambaformer_b200 import _native, autotune, synth
+    from oracle import oracle
+
+    rng = np.random.default_rng(41)
+    ref = synth.random_reference(100_000, rng)
+    qs, ts, hbs = [], [], []
+    for L, hb in ((3000, 300), (3000, 150)):  # a 4-warp and a 2-warp cooperative pair
+        s = int(rng.integers(1000, 90_000))
+        qs.append(synth.apply_errors(ref[s: s + L], synth.ONT, rng))
+        ts.append(ref[s - 100: s + L + 100])
+        hbs.append(hb)
+    ps = synth.PairSet.from_lists(qs, ts, np.array(hbs, np.int32), 100)
+    params = ext.sw_params(2, 4, 4, 2, 0)
+    autotune.set_tuning(autotune.DEFAULT, "cuda:0")
+    lib = _native.lib()
+    assert lib.gmf_sw_test_coop_wait(256, 1) == _native.GMF_OK
+    try:
+        dp = ext.upload_pairs(ps, "cuda:0")
+        out = ext.launch_banded_sw(dp, params)
+        torch.cuda.synchronize()
+        assert int(out.error_flags.item()) & _native.GMF_SWF_TIMEOUT
+        with pytest.raises(RuntimeError, match="bounded wait"):
+            ext.align_pairs(ps, params)
+    finally:
+        assert lib.gmf_sw_test_coop_wait(0, 0) == _native.GMF_OK
+    res = ext.align_pairs(ps, params)
+    want = oracle.sw_batch(qs, ts, ps.half_band, ps.band_offset, 2, 4, 4, 2, 0, threads=2)
+    assert_sw_equal(res, want, label="after the timeout")
