@@ -281,7 +281,7 @@ def run_b200(args):
 
     from graphmambaformer_b200 import chaining, extension
     from graphmambaformer_b200.config import ChainingConfig
-    from graphmambaformer_b200.session import ChainSession, ExtensionSession
+    from graphmambaformer_b200.session import ChainSession, ExtensionSession, pin_anchors
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -503,13 +503,14 @@ def run_b200(args):
         c_ms = max_over_ranks(float(np.mean(cms)))
         anchors_total = sum_over_ranks(float(cb.n_anchors))
         csess = ChainSession(cfg, device)
+        pcb = pin_anchors(cb)  # the batch as a service holds it: page-locked host columns
         for _ in range(2):
-            csess.chain(cb)
+            csess.chain(pcb)
         barrier()
         ce = []
         for _ in range(max(2, args.steps // 4)):
             t0 = time.perf_counter()
-            csess.chain(cb)
+            csess.chain(pcb)
             ce.append((time.perf_counter() - t0) * 1e3)
         barrier()
         ce_ms = max_over_ranks(float(np.mean(ce)))
@@ -679,12 +680,22 @@ def wfa_leg(args, device, stream, flush, seed: int, warm: int) -> dict:
         astep()
     torch.cuda.synchronize(device)
     a_ms = float(np.mean(time_device(astep, max(2, args.steps // 2), stream, flush)))
+    # end to end: the pairs as page-locked CSR arrays (WfaBatch) in, distances and CIGARs out
+    wb = wfa.WfaBatch.of(qs, ts).pinned()
+    wfa.align_wfa_batch(wb, md, device=device)
     e = []
     for _ in range(max(2, args.steps // 4)):
         t0 = time.perf_counter()
-        r = wfa.align_wfa_pairs(qs, ts, md, device=device)
+        r = wfa.align_wfa_batch(wb, md, device=device)
         e.append((time.perf_counter() - t0) * 1e3)
     e_ms = float(np.mean(e))
+    # the same from Python lists of per-pair arrays (the reference's calling form)
+    el = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        wfa.align_wfa_pairs(qs, ts, md, device=device)
+        el.append((time.perf_counter() - t0) * 1e3)
+    el_ms = float(np.mean(el))
     n = len(qs)
     bases = int(sum(len(q) + len(t) for q, t in zip(qs, ts)))
     hist = int(np.sum(np.where(h_dist >= 0, (h_dist.astype(np.int64) + 1) ** 2, 0)))
@@ -695,7 +706,10 @@ def wfa_leg(args, device, stream, flush, seed: int, warm: int) -> dict:
         "e2e": {"value": n / (e_ms * 1e-3), "unit": "alignments/s", "ms_per_step": e_ms,
                 "h2d_bytes_per_step": bases + 16 * (n + 1),
                 # distances, op counts, CIGAR starts and lengths, two counters, the CIGAR words
-                "d2h_bytes_per_step": 32 * n + 12 + 4 * int(len(r.cigar_words))},
+                "d2h_bytes_per_step": 32 * n + 12 + 4 * int(len(r.cigar_words)),
+                "timing": "align_wfa_batch on page-locked CSR pairs",
+                "from_lists": {"value": n / (el_ms * 1e-3), "ms_per_step": el_ms,
+                               "timing": "align_wfa_pairs on Python lists of per-pair arrays"}},
         "config": {"workload": "wfa_pairs_mixed", "pairs": n, "read_len": "lognormal(7.0, 1.2) clipped to 150-20000",
                    "profiles": "Illumina / HiFi / ONT thirds", "target": "the read's source stretch",
                    "max_distance": md, "bases": bases, "mean_distance": float(h_dist[h_dist >= 0].mean()),
@@ -724,19 +738,23 @@ def wfa_leg(args, device, stream, flush, seed: int, warm: int) -> dict:
 
 def sam_records_workload(n: int, seed: int):
     """Alignment records of mixed-length reads (150 bp - 20 kb, both
-    strands, soft clips, every 31st unmapped) with their reads."""
+    strands, soft clips, every 31st unmapped) with their reads, as objects
+    (ReadAlignments, reads with seq / quals / modality) and as arrays
+    (RecordTable, names, ASCII bases, qualities, offsets)."""
     from types import SimpleNamespace
 
-    from graphmambaformer_b200.records import AlignmentRecord, ReadAlignments
+    from graphmambaformer_b200.records import OPS, AlignmentRecord, ReadAlignments, RecordTable
 
     rng = np.random.default_rng(seed)
     lens = np.clip(rng.lognormal(7.0, 1.2, size=n), 150, 20_000).astype(np.int64)
     pool = rng.choice(np.frombuffer(b"ACGT", np.uint8), size=int(lens.sum()))
+    qual = np.zeros(int(lens.sum()), np.uint8)
     results, reads, o = [], [], 0
+    cols = {k: [] for k in ("ref_id", "ref_start", "ref_end", "strand", "mapq")}
+    words, nwords = [], []
     for i, L in enumerate(lens):
         L = int(L)
         seq = pool[o: o + L].tobytes().decode()
-        o += L
         cl, cr = int(rng.integers(0, 40)), int(rng.integers(0, 40))
         mid = L - cl - cr
         cigar = [("S", cl), ("=", mid // 3), ("X", 1), ("=", mid // 3), ("I", 2), ("=", mid - 2 * (mid // 3) - 3),
@@ -746,11 +764,29 @@ def sam_records_workload(n: int, seed: int):
         rec = AlignmentRecord(read_id=f"read{i}", read_len=L, ref_id=0, ref_start=rs, ref_end=rs + mid,
                               strand=1 if i % 2 else -1, mapq=int(rng.integers(0, 61)), cigar=cigar,
                               is_mapped=i % 31 != 0)
+        q = rng.integers(0, 60, size=L) if i % 4 == 0 else None
+        if q is not None:
+            qual[o: o + L] = q
+        o += L
         results.append(ReadAlignments(read_id=rec.read_id, read_len=L, records=[rec]))
-        reads.append(SimpleNamespace(read_id=rec.read_id, seq=seq,
-                                     quals=rng.integers(0, 60, size=L).tolist() if i % 4 == 0 else None,
+        reads.append(SimpleNamespace(read_id=rec.read_id, seq=seq, quals=q.tolist() if q is not None else None,
                                      modality="ont"))
-    return results, reads
+        w = [(m << 4) | OPS.index(op) for op, m in cigar] if rec.is_mapped else []
+        words.extend(w)
+        nwords.append(len(w))
+        for k, v in (("ref_id", 0 if rec.is_mapped else -1), ("ref_start", rs), ("ref_end", rs + mid),
+                     ("strand", rec.strand), ("mapq", rec.mapq)):
+            cols[k].append(v)
+    woff = np.zeros(n + 1, np.int64)
+    np.cumsum(nwords, out=woff[1:])
+    seq_off = np.zeros(n + 1, np.int64)
+    np.cumsum(lens, out=seq_off[1:])
+    table = RecordTable(read=np.arange(n, dtype=np.int64), ref_id=np.array(cols["ref_id"], np.int64),
+                        ref_start=np.array(cols["ref_start"], np.int64), ref_end=np.array(cols["ref_end"], np.int64),
+                        strand=np.array(cols["strand"], np.int8), mapq=np.array(cols["mapq"], np.int32),
+                        is_primary=np.ones(n, bool), cigar=np.array(words, np.uint32), cigar_off=woff)
+    arrays = dict(table=table, names=[r.read_id for r in reads], seq=pool, seq_off=seq_off, qual=qual)
+    return results, reads, arrays
 
 
 def sam_leg(args, device, stream, flush, warm: int) -> dict:
@@ -765,12 +801,28 @@ def sam_leg(args, device, stream, flush, warm: int) -> dict:
 
     from graphmambaformer_b200 import _native
     from graphmambaformer_b200.device import to_device
-    from graphmambaformer_b200.records import render_sam, sam_records
+    from graphmambaformer_b200.records import render_sam, render_sam_array, sam_batch, sam_records
 
-    results, reads = sam_records_workload(args.sam_records, seed=9)
+    results, reads, arrays = sam_records_workload(args.sam_records, seed=9)
     t0 = time.perf_counter()
     b = sam_records(results, reads, "ont", False, {0: 10 ** 9})
     layout_ms = (time.perf_counter() - t0) * 1e3
+    # the same records held as arrays: bases and qualities in page-locked memory, as a service keeps them
+    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
+    seq_p, qual_p = pin(arrays["seq"]), pin(arrays["qual"])
+
+    def table_layout():
+        return sam_batch(arrays["table"], arrays["names"], seq_p, arrays["seq_off"], qual_p, "ont", False,
+                         {0: 10 ** 9})
+
+    bt = table_layout()
+    for f in ("names", "name_off", "seq", "seq_off", "qual", "contig", "contig_names", "contig_off", "ref_start",
+              "ref_end", "strand", "mapq", "cigar", "cigar_start", "cigar_len", "tags", "tag_off"):
+        if not np.array_equal(getattr(bt, f), getattr(b, f)):
+            raise RuntimeError(f"the array layout differs from the object layout in {f}")
+    t0 = time.perf_counter()
+    table_layout()
+    table_layout_ms = (time.perf_counter() - t0) * 1e3
     n = len(b)
     d = {k: to_device(getattr(b, k), device) for k in ("names", "name_off", "seq", "seq_off", "qual", "contig",
                                                         "contig_names", "contig_off", "ref_start", "ref_end",
@@ -808,12 +860,20 @@ def sam_leg(args, device, stream, flush, warm: int) -> dict:
     h2d = int(sum(getattr(b, k).nbytes for k in ("names", "name_off", "seq", "seq_off", "qual", "contig",
                                                   "contig_names", "contig_off", "ref_start", "ref_end", "strand",
                                                   "mapq", "cigar", "cigar_start", "cigar_len", "tags", "tag_off")))
+    keep = [render_sam_array(table_layout(), device) for _ in range(2)]  # both page-locked text buffers made
+    del keep
     e = []
     for _ in range(max(2, args.steps // 4)):
         t0 = time.perf_counter()
-        out = render_sam(b, device)
+        out = render_sam_array(table_layout(), device)
         e.append((time.perf_counter() - t0) * 1e3)
     e_ms = float(np.mean(e))
+    eb = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        render_sam(b, device)
+        eb.append((time.perf_counter() - t0) * 1e3)
+    eb_ms = float(np.mean(eb))
     res = {
         "value": n / (ms * 1e-3), "unit": "records/s", "ms_per_step": ms,
         "text_gb_per_s": total / (ms * 1e-3) / 1e9,
@@ -821,8 +881,12 @@ def sam_leg(args, device, stream, flush, warm: int) -> dict:
                      "bytes_per_step": alg, "text_bytes": total},
         "e2e": {"value": n / (e_ms * 1e-3), "unit": "records/s", "ms_per_step": e_ms,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": len(out),
-                "timing": "render_sam: host arrays in, SAM bytes out"},
+                "timing": "sam_batch + render_sam_array: record table and page-locked read columns in, "
+                          "SAM text out in page-locked memory",
+                "from_layout_bytes": {"value": n / (eb_ms * 1e-3), "ms_per_step": eb_ms,
+                                      "timing": "render_sam on a ready layout, text as bytes"}},
         "host_layout_ms": layout_ms,
+        "table_layout_ms": table_layout_ms,
         "config": {"workload": "sam_records_mixed", "records": n, "bases": int(b.seq.size),
                    "read_len": "lognormal(7.0, 1.2) clipped to 150-20000", "strands": "alternating",
                    "qualities": "every 4th read", "unmapped": "every 31st"},
@@ -1181,10 +1245,12 @@ def compact_summary(line: dict) -> dict:
             s["long_reads"]["wide_max_half_band"] = lr["wide_sw"]["max_half_band"]
     wf = line.get("wfa")
     if wf:
-        s["wfa"] = {"aln_s": _r(wf["value"]), "e2e_aln_s": _r(wf.get("e2e", {}).get("value"))}
+        s["wfa"] = {"aln_s": _r(wf["value"]), "e2e_aln_s": _r(wf.get("e2e", {}).get("value")),
+                    "lists_aln_s": _r(wf.get("e2e", {}).get("from_lists", {}).get("value"))}
     sa = line.get("sam")
     if sa:
-        s["sam"] = {"records_s": _r(sa["value"]), "e2e_records_s": _r(sa.get("e2e", {}).get("value"))}
+        s["sam"] = {"records_s": _r(sa["value"]), "e2e_records_s": _r(sa.get("e2e", {}).get("value")),
+                    "e2e_ms": _r(sa.get("e2e", {}).get("ms_per_step"), 3), "table_layout_ms": _r(sa.get("table_layout_ms"), 3)}
     if line.get("parity"):
         s["parity"] = {k: line["parity"][k] for k in ("pairs", "mismatches")}
     cb = line.get("cpu_baseline")

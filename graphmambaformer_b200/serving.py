@@ -65,18 +65,21 @@ class BatchAlignments:
 
     def __init__(self, n_reads: int, chain_off: np.ndarray, cols: Optional[dict] = None,
                  words: Optional[np.ndarray] = None, objects: Optional[list] = None, lo: int = 0,
-                 hi: Optional[int] = None):
+                 hi: Optional[int] = None, chains: Optional[dict] = None):
         self.n_reads = int(n_reads)
         self.chain_off = chain_off  # n_reads + 1: the chains of read r are chain_off[r] .. chain_off[r+1]-1
         self.cols = cols            # per chain: score, qs, qe, ts, te, counts (C, 4), cstart, clen, clip_l, clip_r
         self.words = words          # CIGAR words (run << 4 | op), without the soft clips
         self.objects = objects      # or per chain, ready ExtensionResults (the WFA path)
+        self.chains = chains        # per chain: the chain's score (f64), strand and primary flag
         self.lo = int(lo)
         self.hi = self.n_reads if hi is None else int(hi)
 
     @staticmethod
     def empty(n_reads: int) -> "BatchAlignments":
-        return BatchAlignments(n_reads, np.zeros(n_reads + 1, np.int64), objects=[])
+        z = np.zeros(0, np.int32)
+        return BatchAlignments(n_reads, np.zeros(n_reads + 1, np.int64), objects=[],
+                               chains=dict(score=np.zeros(0), strand=z, prim=z))
 
     def __len__(self) -> int:
         return self.hi - self.lo
@@ -102,7 +105,7 @@ class BatchAlignments:
             if step != 1:
                 raise ValueError("BatchAlignments slices take consecutive reads")
             return BatchAlignments(self.n_reads, self.chain_off, self.cols, self.words, self.objects,
-                                   self.lo + a, self.lo + max(a, b))
+                                   self.lo + a, self.lo + max(a, b), self.chains)
         if i < 0:
             i += len(self)
         if not 0 <= i < len(self):
@@ -194,7 +197,7 @@ class BatchAligner:
         dl = self.buf.download
         h = {k: dl("h_" + k, t, n, s) for k, t, n in
              (("n", o["n"], R), ("strand", o["strand"], R * mc), ("span", o["span"], 4 * R * mc),
-              ("spread", spread_d, R * mc))}
+              ("spread", spread_d, R * mc), ("score", o["score"], R * mc), ("prim", o["prim"], R * mc))}
         s.synchronize()
         n_ch = np.minimum(h["n"][:R].numpy(), mc)
         strand = h["strand"][: R * mc].numpy().reshape(R, mc)
@@ -209,12 +212,15 @@ class BatchAligner:
         if C == 0:
             return BatchAlignments.empty(R)
         spread = spread_all[cr, ck].astype(np.int64)
+        chains = dict(score=h["score"][: R * mc].numpy().reshape(R, mc)[cr, ck],
+                      strand=strand[cr, ck].copy(), prim=h["prim"][: R * mc].numpy().reshape(R, mc)[cr, ck])
         rc = strand[cr, ck] < 0
         sp4 = span[cr, ck].astype(np.int64)  # read_start, read_end, ref_start, ref_end
         if self.ecfg.algorithm == "wfa":
-            return BatchAlignments(R, chain_off, objects=self._extend_wfa(R, rl, roff, reads_d, cr, rc, sp4, spread))
+            return BatchAlignments(R, chain_off, objects=self._extend_wfa(R, rl, roff, reads_d, cr, rc, sp4, spread),
+                                   chains=chains)
         cols, words = self._extend_sw(R, rl, roff, reads_d, cr, rc, sp4, spread, shared=True)
-        return BatchAlignments(R, chain_off, cols, words)
+        return BatchAlignments(R, chain_off, cols, words, chains=chains)
 
     def _gather(self, tag: str, reads_d, roff, rl, cr, rc, wstart, wlen) -> tuple:
         """Queries (reverse-complemented for strand -1) and reference

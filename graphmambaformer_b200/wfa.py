@@ -102,6 +102,75 @@ def upload_wfa_pairs(queries: Sequence[np.ndarray], targets: Sequence[np.ndarray
     return DeviceWfaPairs(len(queries), q, qo, t, to, ql, tl, dev)
 
 
+@dataclass
+class WfaBatch:
+    """Host pairs as CSR code arrays: pair b is ``query[query_off[b]:
+    query_off[b+1]]`` against ``target[target_off[b]: target_off[b+1]]``
+    (int8 codes, int64 offsets).  Code arrays in page-locked memory (see
+    :meth:`pinned`) go to the device without a host copy."""
+
+    query: np.ndarray
+    query_off: np.ndarray
+    target: np.ndarray
+    target_off: np.ndarray
+
+    def __len__(self) -> int:
+        return len(self.query_off) - 1
+
+    @staticmethod
+    def of(queries: Sequence[np.ndarray], targets: Sequence[np.ndarray]) -> "WfaBatch":
+        if len(queries) != len(targets):
+            raise ValueError("queries and targets differ in number")
+
+        def csr(seqs):
+            off = np.zeros(len(seqs) + 1, np.int64)
+            np.cumsum(np.fromiter((len(x) for x in seqs), np.int64, len(seqs)), out=off[1:])
+            codes = np.empty(int(off[-1]), np.int8)
+            if len(codes):
+                np.concatenate(seqs, out=codes, casting="unsafe")
+            return codes, off
+
+        q, qo = csr(queries)
+        t, to = csr(targets)
+        return WfaBatch(q, qo, t, to)
+
+    def pinned(self) -> "WfaBatch":
+        """A copy whose code arrays live in page-locked host memory."""
+
+        def pin(a):
+            h = torch.empty(max(len(a), 1), dtype=torch.int8, pin_memory=True)
+            h[: len(a)].copy_(torch.from_numpy(np.ascontiguousarray(a, np.int8)))
+            return h.numpy()[: len(a)]
+
+        return WfaBatch(pin(self.query), self.query_off.copy(), pin(self.target), self.target_off.copy())
+
+
+def upload_wfa_batch(batch: WfaBatch, device=None) -> DeviceWfaPairs:
+    """The CSR pairs on the device (copies enqueued on the current stream; a
+    page-locked code array must stay unchanged until they have run)."""
+    dev = require_cuda(device)
+    qo, to = np.asarray(batch.query_off, np.int64), np.asarray(batch.target_off, np.int64)
+    if len(qo) != len(to) or len(qo) < 1 or qo[0] != 0 or to[0] != 0:
+        raise ValueError("query_off and target_off must be offset arrays of the same batch, starting at 0")
+    ql, tl = np.diff(qo), np.diff(to)
+    if len(ql) and (ql.min() < 0 or tl.min() < 0):
+        raise ValueError("offsets must not decrease")
+    if len(ql) and max(ql.max(), tl.max()) > (1 << 28):
+        raise ValueError("sequence longer than the library's limit (2^28 codes)")
+    if len(batch.query) < qo[-1] or len(batch.target) < to[-1]:
+        raise ValueError("offsets run past the code arrays")
+
+    def codes(a, n):
+        a = np.asarray(a)[:n]
+        if a.dtype != np.int8:
+            a = a.astype(np.int8)
+        return to_device(a, dev) if n else torch.zeros(1, dtype=torch.int8, device=dev)
+
+    return DeviceWfaPairs(len(ql), codes(batch.query, int(qo[-1])), to_device(qo, dev),
+                          codes(batch.target, int(to[-1])), to_device(to, dev), ql.astype(np.int32),
+                          tl.astype(np.int32), dev)
+
+
 def _check_bound(max_distance: int, max_len: int) -> int:
     """The bound the device call takes.  No distance exceeds the longer side,
     so a bound above it changes nothing, and a negative bound acts like 0
@@ -214,6 +283,31 @@ def align_wfa_pairs(queries: Sequence[np.ndarray], targets: Sequence[np.ndarray]
     return align_device_pairs(dp, max_distance, traceback=traceback, history_budget=history_budget)
 
 
+def align_wfa_batch(batch: WfaBatch, max_distance: int = 4096, traceback: bool = True, device=None,
+                    history_budget: int = HISTORY_BUDGET) -> WfaResult:
+    """:func:`align_wfa_pairs` for pairs already laid out as CSR arrays."""
+    dev = require_cuda(device)
+    stream = torch.cuda.current_stream(dev)
+    with torch.cuda.stream(stream):
+        dp = upload_wfa_batch(batch, dev)
+    return align_device_pairs(dp, max_distance, stream=stream, traceback=traceback, history_budget=history_budget)
+
+
+def history_chunks(hist: np.ndarray, budget: int) -> list:
+    """Consecutive ranges [s, e) of pairs whose history entries sum to at
+    most ``budget`` each, taken greedily in order; a pair above the budget
+    forms a range of its own."""
+    n = len(hist)
+    cum = np.zeros(n + 1, np.int64)
+    np.cumsum(hist, out=cum[1:])
+    bounds = [0]
+    while bounds[-1] < n:
+        s = bounds[-1]
+        e = int(np.searchsorted(cum, cum[s] + budget, side="right")) - 1
+        bounds.append(max(e, s + 1))
+    return [(bounds[k], bounds[k + 1]) for k in range(len(bounds) - 1)]
+
+
 def align_device_pairs(dp: DeviceWfaPairs, max_distance: int = 4096, stream: Optional[torch.cuda.Stream] = None,
                        traceback: bool = True, history_budget: int = HISTORY_BUDGET, workspace=None) -> WfaResult:
     """Pairs already on the device in, host wavefront alignments out (on
@@ -244,17 +338,9 @@ def _align_device(dp, max_distance, stream, sp, traceback, history_budget, works
     # chunks whose histories fit the budget (a pair above it alone)
     hist = np.where((h_dist >= 0) & (dp.h_qlen > 0) & (dp.h_tlen > 0),
                     (h_dist.astype(np.int64) + 1) ** 2, 0)
-    chunks, cur, acc = [], [], 0
-    for p in range(dp.n):
-        if cur and acc + hist[p] > history_budget:
-            chunks.append(cur)
-            cur, acc = [], 0
-        cur.append(p)
-        acc += int(hist[p])
-    if cur:
-        chunks.append(cur)
-    for ch in chunks:
-        idx = np.asarray(ch, np.int64)
+    chunks = history_chunks(hist, history_budget)
+    for c0, c1 in chunks:
+        idx = np.arange(c0, c1, dtype=np.int64)
         if len(chunks) == 1:
             sub, d_sub, h_d = dp, dist_d, h_dist
         else:

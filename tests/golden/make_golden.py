@@ -55,6 +55,12 @@ Fixtures:
   sorted anchor segments over random graphs (several hop limits, lookbacks,
   bonus weights, the legacy linear blend, duplicated anchor keys, transition
   keys that are not in the segment).
+* ``pipeline_golden.pkl`` -- ``FastAlignmentPipeline.align`` end to end
+  with its stock CPU stage objects (minimizer seeding, ``AffineChainer``,
+  ``ExtensionEngine`` in both algorithms, margin MAPQ, records) on seeded
+  reads: HiFi, ONT and 150 bp reads on both strands, chimeric and repeated
+  reads with secondary chains, unmappable reads, a reference with an N run.
+  Stored per read: the seed stage's anchors, the chains and the records.
 """
 
 from __future__ import annotations
@@ -983,6 +989,70 @@ def make_sam(rng):
           f"{len(out[(True, None)]['segments'])} segments with secondaries")
 
 
+def make_pipeline(rng):
+    """``FastAlignmentPipeline.align`` (pipeline.py L438-512) with its stock
+    stage objects on the CPU: minimizer seeding (k=15, w=10), AffineChainer
+    (chain_dp_numpy, f64), ExtensionEngine in both algorithms, margin MAPQ
+    and records.  Stored per read: the seed stage's anchors (the input a
+    drop-in chainer receives), the chains, the extensions and the records."""
+    import pickle
+
+    from graphmambaformer.alignment.pipeline import FastAlignmentPipeline
+    from graphmambaformer.config import AccelConfig, PipelineConfig, SeedingConfig
+
+    ref = synth.random_reference(400_000, rng)
+    ref[200_000:200_050] = 5  # an N run
+    ref_str = synth.decode_bases(ref)
+    reads, ids = [], []
+    for r in range(28):
+        kind = r % 7
+        if kind == 6:  # nothing to map
+            read = synth.random_reference(int(rng.integers(300, 2000)), rng)
+        else:
+            prof = (synth.HIFI, synth.ONT, synth.ILLUMINA)[kind % 3]
+            L = 150 if prof is synth.ILLUMINA else int(rng.integers(1500, 6000))
+            s0 = int(rng.integers(0, len(ref) - L))
+            tmpl = ref[s0: s0 + L]
+            read = synth.apply_errors(tmpl if r % 2 else synth.reverse_complement(tmpl), prof, rng)
+            if kind == 4:  # chimeric: a second locus joined on, for secondary chains
+                s1 = int(rng.integers(0, len(ref) - 1500))
+                read = np.concatenate([read, synth.apply_errors(ref[s1: s1 + 1500], synth.HIFI, rng)])
+            if kind == 5:  # a repeated stretch, mapped at two places
+                read = np.concatenate([read, read[: min(len(read), 800)]])
+        reads.append(synth.decode_bases(read))
+        ids.append(f"r{r}")
+    runs = {}
+    for algorithm in ("banded_sw", "wfa"):
+        cfg = PipelineConfig(mode="fast", seeding=SeedingConfig(modes=("minimizer",)),
+                             extension=ExtensionConfig(algorithm=algorithm),
+                             accel=AccelConfig(device="cpu", num_workers=1, apply_global_switches=False))
+        pipe = FastAlignmentPipeline(cfg, device="cpu")
+        index = pipe.build_reference(ref_str)
+        results, _ = pipe.align(reads, index, read_ids=ids)
+        per = []
+        for res in results:
+            a = res.anchors
+            per.append(dict(
+                anchors=np.stack([a.read_pos, a.ref_pos, a.length, a.strand.astype(np.int64)], 1)
+                if len(a) else np.zeros((0, 4), np.int64),
+                chains=[dict(anchor_idx=np.asarray(c.anchor_idx, np.int64), score=float(c.score), strand=int(c.strand),
+                             span=(int(c.read_start), int(c.read_end), int(c.ref_start), int(c.ref_end)),
+                             is_primary=bool(c.is_primary)) for c in res.chains],
+                records=[dict(ref_id=int(x.ref_id), ref_start=int(x.ref_start), ref_end=int(x.ref_end),
+                              strand=int(x.strand), mapq=int(x.mapq), chain_score=float(x.chain_score),
+                              alignment_score=float(x.alignment_score), cigar=[(op, int(n)) for op, n in x.cigar],
+                              is_mapped=bool(x.is_mapped), is_primary=bool(x.is_primary),
+                              is_supplementary=bool(x.is_supplementary), n_anchors=int(x.n_anchors),
+                              n_chains=int(x.n_chains), node_id=int(x.node_id)) for x in res.records]))
+        runs[algorithm] = dict(config=dict(chaining=vars(cfg.chaining).copy(), extension=vars(cfg.extension).copy()),
+                               reads=per)
+        n_rec = sum(len(x["records"]) for x in per)
+        n_map = sum(1 for x in per for y in x["records"] if y["is_mapped"])
+        print(f"pipeline_golden.pkl [{algorithm}]: {len(per)} reads, {n_rec} records, {n_map} mapped")
+    with open(os.path.join(HERE, "pipeline_golden.pkl"), "wb") as fh:
+        pickle.dump(dict(ref=ref, reads=reads, ids=ids, runs=runs), fh, protocol=4)
+
+
 if __name__ == "__main__":
     which = sys.argv[1:] or ["sw", "chain", "extend", "hybrid"]
     if "sw" in which:
@@ -1003,3 +1073,5 @@ if __name__ == "__main__":
         make_xdrop(np.random.default_rng(707))
     if "sam" in which:
         make_sam(np.random.default_rng(808))
+    if "pipeline" in which:
+        make_pipeline(np.random.default_rng(1010))

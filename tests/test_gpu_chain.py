@@ -275,14 +275,16 @@ def test_empty_reads_and_single_strand(chaining):
     assert len(out[1]) == 1 and out[1][0].strand == -1 and list(out[1][0].anchor_idx) == [0, 1, 2]
 
 
+@pytest.mark.parametrize("pinned", [False, True])
 @pytest.mark.parametrize("chunks", [None, 1, 3, 7])
-def test_chain_session_host_batches_in_runs(chaining, chunks):
+def test_chain_session_host_batches_in_runs(chaining, chunks, pinned):
     """The host-buffer session (the e2e path): a batch split into runs of
-    whole reads, staged and copied out while the previous run chains, gives
-    the oracle's chains; so does a second call reusing the buffers."""
+    whole reads, staged (or, with page-locked columns, copied directly) while
+    the previous run chains, gives the oracle's chains; so does a second call
+    reusing the buffers, which leaves the first call's result untouched."""
     from graphmambaformer_b200 import synth
     from graphmambaformer_b200.config import ChainingConfig
-    from graphmambaformer_b200.session import ChainSession
+    from graphmambaformer_b200.session import ChainSession, pin_anchors
     from oracle import oracle
 
     batch = synth.chaining_reads_hifi(n_reads=60, seed=77, ref_len=2_000_000, mean_len=5000)
@@ -290,8 +292,13 @@ def test_chain_session_host_batches_in_runs(chaining, chunks):
     want = oracle.chain_batch(batch.read_off, batch.read_pos, batch.ref_pos, batch.length, batch.strand,
                               oracle.penalty_lut(5000, 6.0, 0.05, 0.5), max_lookback=50, threads=8)
     sess = ChainSession(cfg, "cuda:0")
-    for _ in range(2):
-        got = sess.chain(batch, chunks=chunks)
+    src = pin_anchors(batch) if pinned else batch
+    if pinned:
+        import torch
+
+        assert torch.from_numpy(src.read_pos).is_pinned()
+    results = [sess.chain(src, chunks=chunks) for _ in range(2)]
+    for got in results:
         assert np.array_equal(got.n_chains, want.n_chains)
         for r in range(len(batch)):
             for a, b in zip(got.chains(r), want.chains(batch.read_off, r)):

@@ -164,3 +164,56 @@ def test_device_seeding_with_concurrent_workers(pool):
         one.stop()
         many.stop()
     assert many.batches > 3
+
+
+@pytest.mark.parametrize("algorithm", ["banded_sw", "wfa"])
+def test_batch_record_table_and_sam_match_object_path(pool, algorithm):
+    """The serving batch's records built as arrays (record_table over the
+    chain and extension columns) equal the fast pipeline's per-read records
+    from the stage objects (read_alignments over AffineChainer +
+    ExtensionEngine), and their SAM text (sam_batch + render) equals the
+    object path's (sam_records + render), secondaries included or not."""
+    import torch
+
+    from graphmambaformer_b200 import synth
+    from graphmambaformer_b200.chaining import AffineChainer, ChainingConfig
+    from graphmambaformer_b200.config import ExtensionConfig
+    from graphmambaformer_b200.extension import ExtensionEngine
+    from graphmambaformer_b200.records import read_alignments, record_table, render_sam, sam_batch, sam_records
+    from graphmambaformer_b200.serving import BatchAligner
+    from graphmambaformer_b200.types import AnchorSet, words_to_cigar
+
+    idx = np.arange(70)
+    reads, anchors = pool.take(idx)
+    ccfg, ecfg = ChainingConfig(), ExtensionConfig(algorithm=algorithm)
+    ref_d = torch.from_numpy(pool.ref).to("cuda:0")
+    ba = BatchAligner(ref_d, "cuda:0", ccfg, ecfg).align(reads, anchors)
+    table = record_table(ba)
+    sets = []
+    for r in range(len(reads)):
+        rp, fp, ln, st = anchors.read(r)
+        sets.append(AnchorSet.from_lists(rp, fp, ln, st, read_len=len(reads[r]), ref_len=len(pool.ref)))
+    chains = AffineChainer(ccfg, device="cuda:0").chain_batch(sets)
+    exts = ExtensionEngine(ecfg, device="cuda:0").extend_batch(
+        [synth.decode_bases(x) for x in reads], chains, sets, synth.decode_bases(pool.ref))
+    names = [f"q{r}" for r in range(len(reads))]
+    objs = [read_alignments(names[r], len(reads[r]), sets[r], chains[r], exts[r]) for r in range(len(reads))]
+    recs = [rec for ra in objs for rec in ra.records]
+    assert len(recs) == len(table)
+    assert any(not x.is_mapped for x in recs) == bool((table.ref_id < 0).any())
+    for i, rec in enumerate(recs):
+        assert (table.ref_id[i] >= 0) == rec.is_mapped, i
+        if rec.is_mapped:
+            assert (table.ref_start[i], table.ref_end[i], table.strand[i], table.mapq[i], bool(table.is_primary[i])) \
+                == (rec.ref_start, rec.ref_end, rec.strand, rec.mapq, rec.is_primary), i
+            assert words_to_cigar(table.cigar[table.cigar_off[i]: table.cigar_off[i + 1]]) == \
+                [tuple(x) for x in rec.cigar], i
+    seq_off = np.zeros(len(reads) + 1, np.int64)
+    np.cumsum([len(x) for x in reads], out=seq_off[1:])
+    codes = np.concatenate(reads).astype(np.int8)
+    texts = [synth.decode_bases(x) for x in reads]
+    refs = {0: len(pool.ref)}
+    for secondary in (False, True):
+        want = render_sam(sam_records(objs, texts, "ont", secondary, refs))
+        got = render_sam(sam_batch(table, names, codes, seq_off, None, "ont", secondary, refs))
+        assert got == want and len(got) > 0

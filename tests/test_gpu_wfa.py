@@ -174,3 +174,38 @@ def test_wfa_spilled_wavefronts_and_chunked_histories_match_oracle():
             assert sum(n for op, n in got if op in "=XI") == len(qs[b])
             assert sum(n for op, n in got if op in "=XD") == len(ts[b])
             assert sum(n for op, n in got if op in "XID") == d
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+def test_csr_batch_matches_list_form_and_oracle(pinned):
+    """align_wfa_batch on the pairs as CSR arrays (plain, or page-locked and
+    copied to the device directly) gives the list form's distances and
+    CIGARs, and the oracle's; empty sides and a bound some pairs exceed
+    included."""
+    from oracle import oracle
+
+    from graphmambaformer_b200 import synth
+    from graphmambaformer_b200.wfa import WfaBatch, align_wfa_batch, align_wfa_pairs
+
+    rng = np.random.default_rng(23)
+    qs, ts = [], []
+    for L in (0, 1, 7, 150, 600, 2500):
+        for _ in range(2):
+            a = synth.random_reference(L, rng).astype(np.int8)
+            qs.append(a)
+            ts.append(synth.apply_errors(a, synth.ONT, rng).astype(np.int8) if L else a.copy())
+    qs.append(np.zeros(0, np.int8))
+    ts.append(synth.random_reference(30, rng).astype(np.int8))
+    md = 90
+    batch = WfaBatch.of(qs, ts)
+    if pinned:
+        batch = batch.pinned()
+    got = align_wfa_batch(batch, md)
+    ref = align_wfa_pairs(qs, ts, md)
+    assert np.array_equal(got.distance, ref.distance)
+    assert (got.distance < 0).any() and (got.distance >= 0).any()
+    for b in range(len(qs)):
+        d, cigar = oracle.wfa_align(qs[b], ts[b], md)
+        assert int(got.distance[b]) == d, b
+        if d >= 0:
+            assert got.cigar(b) == ref.cigar(b) == cigar, b

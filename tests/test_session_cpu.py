@@ -27,8 +27,8 @@ def test_run_cuts_partition_the_reads(chunks):
             continue
         assert cut[0] == 0 and cut[-1] == R and np.all(np.diff(cut) > 0)
         C = len(cut) - 1
-        want = chunks if chunks is not None else min(4, max(1, A // 2_000_000))
+        want = chunks if chunks is not None else min(2, max(1, A // 2_000_000))
         assert C <= max(1, min(want, R))
         per_run = np.diff(off[cut])
         assert per_run.max() <= A / C + np.diff(off).max()
-    assert len(run_cuts(cases[-1], None)) - 1 == 4
+    assert len(run_cuts(cases[-1], None)) - 1 == 2

@@ -10,6 +10,7 @@ from __future__ import annotations
 from types import SimpleNamespace
 
 import numpy as np
+import pytest
 
 from helpers import load, words_to_cigar
 from oracle import oracle
@@ -67,3 +68,43 @@ def test_wfa_mode_windows_through_the_oracle_match_reference_golden():
             assert [got.n_match, got.n_mismatch, got.n_insertion, got.n_deletion] == list(g["x_counts"][kk]), kk
         k += len(chains)
     assert k == len(g["x_score"]) and n_wfa > 0 and n_fallback > 0
+
+
+def test_history_chunks_follow_the_greedy_split():
+    """history_chunks equals the pair-by-pair greedy split: a range closes
+    before the pair that would take it over the budget, and a pair above
+    the budget stands alone."""
+    from graphmambaformer_b200.wfa import history_chunks
+
+    def greedy(hist, budget):
+        out, cur, acc = [], [], 0
+        for p, h in enumerate(hist):
+            if cur and acc + h > budget:
+                out.append((cur[0], cur[-1] + 1))
+                cur, acc = [], 0
+            cur.append(p)
+            acc += int(h)
+        if cur:
+            out.append((cur[0], cur[-1] + 1))
+        return out
+
+    rng = np.random.default_rng(3)
+    for n in (0, 1, 2, 17, 500):
+        for budget in (1, 50, 1000, 10 ** 9):
+            hist = rng.integers(0, 120, size=n) ** 2 * (rng.random(n) < 0.8)
+            assert history_chunks(hist, budget) == greedy(hist, budget), (n, budget)
+
+
+def test_wfa_batch_csr_layout():
+    from graphmambaformer_b200.wfa import WfaBatch
+
+    rng = np.random.default_rng(4)
+    qs = [rng.integers(0, 4, size=L).astype(np.int8) for L in (0, 3, 9, 0, 5)]
+    ts = [rng.integers(0, 4, size=L).astype(np.int8) for L in (2, 0, 9, 0, 6)]
+    b = WfaBatch.of(qs, ts)
+    assert len(b) == 5 and b.query.dtype == np.int8 and b.query_off.dtype == np.int64
+    for i in range(5):
+        assert np.array_equal(b.query[b.query_off[i]: b.query_off[i + 1]], qs[i])
+        assert np.array_equal(b.target[b.target_off[i]: b.target_off[i + 1]], ts[i])
+    with pytest.raises(ValueError):
+        WfaBatch.of(qs, ts[:2])
