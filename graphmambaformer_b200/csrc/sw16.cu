@@ -183,30 +183,31 @@ __device__ __forceinline__ void chunk16(Cells16& c, const K16& K, const Grp<L>& 
                                         unsigned (&hk)[4], unsigned (&pko)[4]) {
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
-        // Packed adds and subtracts below are plain 32-bit operations: every
-        // operand half is a biased value >= pmax, and every difference is
-        // taken between values known to be ordered, so no half borrows or
-        // carries into the other (a 16x2 __vadd2 / __vsub2 costs about three
-        // instructions on this part).
+        // Every operand half is a biased value >= pmax and every difference
+        // is taken between values known to be ordered, so the per-half adds
+        // and subtracts below never wrap.  They are written as 16x2 adds
+        // (__vadd2 / __vsub2), which issue on the FMA pipe: the DPX maxima,
+        // permutes and logic of the step all take the ALU pipe, which runs
+        // at half rate and bounds the step.
         const unsigned tp = prmt(tw, tpv, tsel(u));
         const unsigned mis = flag2(c.qp ^ tp);  // 0: match, 1: mismatch
-        const unsigned diag = c.hd + K.MATCH2 - mis * K.MX;
-        const unsigned fa = c.hv - K.GO2;
+        const unsigned diag = __vadd2(c.hd, K.MATCH2) - mis * K.MX;  // one multiply-add, no borrow
+        const unsigned fa = __vsub2(c.hv, K.GO2);
         unsigned F = __viaddmax_u16x2(c.fv, K.NGE2, fa);  // max(F above - ext, H above - open)
         unsigned M = __vimax3_u16x2(diag, F, K.Z2);
-        const unsigned ea = c.ml - K.GO2;
+        const unsigned ea = __vsub2(c.ml, K.GO2);
         unsigned E = __viaddmax_u16x2(c.el, K.NGE2, ea);
         unsigned H = umax2(M, E);
         if (TB) {
-            // Each flag is bit 15 of a half of (ordered difference + 0x7fff):
-            // set when the difference is at least 1.  The classifier keeps
-            // every difference within 15 bits, so the sums neither carry nor
-            // borrow across halves.
-            const unsigned n1 = H - diag + 0x7FFF7FFFu;  // H != diag
-            const unsigned n2 = H - F + 0x7FFF7FFFu;     // H != F
-            const unsigned fc = F - fa + 0x7FFF7FFFu;    // F extends (F above - ext > H above - open)
-            unsigned ec = 0u;                            // E extends
-            if (EM == 0) ec = E - ea + 0x7FFF7FFFu;      //   open > ext: E_left - ext > M_left - open
+            // Each flag is bit 15 of a half of (smaller - larger) of an
+            // ordered pair: set when their difference is at least 1.  The
+            // classifier keeps every difference within 15 bits, so a
+            // difference of d >= 1 leaves 2^16 - d >= 2^15 in the half.
+            const unsigned n1 = __vsub2(diag, H);  // H != diag
+            const unsigned n2 = __vsub2(F, H);     // H != F
+            const unsigned fc = __vsub2(fa, F);    // F extends (F above - ext > H above - open)
+            unsigned ec = 0u;                      // E extends
+            if (EM == 0) ec = __vsub2(ea, E);      //   open > ext: E_left - ext > M_left - open
             if (EM == 2) ec = c.el - E + K.EB2;          //   open < ext: E == E_left - ext (ties extend)
             // sign-replicated high bytes: [n1.lo n1.hi n2.lo n2.hi], [fc.lo fc.hi ec.lo ec.hi]
             const unsigned w1 = prmt(n1, n2, 0xFDB9u);
@@ -218,8 +219,8 @@ __device__ __forceinline__ void chunk16(Cells16& c, const K16& K, const Grp<L>& 
             // in-band mask: slot - lo >= 0 and hi - slot >= 0 per half, kept as
             // counters biased by 32768 (they never leave [0, 65535], so plain
             // adds suffice); bit 15 of both set = in band
-            c.ma += ONE2;
-            c.mb -= ONE2;
+            c.ma = __vadd2(c.ma, ONE2);
+            c.mb = __vsub2(c.mb, ONE2);
             const unsigned m = prmt(c.ma & c.mb, 0u, 0xBB99u);  // 0xFFFF per in-band half
             H = (H & m) | (K.Z2 & ~m);
             F = (F & m) | (K.NEG2 & ~m);
@@ -254,8 +255,8 @@ __device__ __forceinline__ void chunk16_any(Cells16& c, const K16& K, const Grp<
                                             unsigned (&hk)[4], unsigned (&pko)[4]) {
     if (__all_sync(FULL_MASK, chunk_in_band(c))) {
         chunk16<L, TB, EM, false>(c, K, grp, src, tw, tpv, from_rv, rv, hk, pko);
-        c.ma += 4u * ONE2;
-        c.mb -= 4u * ONE2;
+        c.ma = __vadd2(c.ma, 4u * ONE2);
+        c.mb = __vsub2(c.mb, 4u * ONE2);
     } else {
         chunk16<L, TB, EM, true>(c, K, grp, src, tw, tpv, from_rv, rv, hk, pko);
     }
@@ -300,8 +301,8 @@ struct BestTrack16 {
     __device__ __forceinline__ void update(unsigned& lb, const unsigned (&hk)[4], int g0) {
         const unsigned nb = __vimax3_u16x2(lb, __vimax3_u16x2(hk[0], hk[1], hk[2]), hk[3]);
         // nb >= lb in each half and the difference stays within 15 bits:
-        // bit 15 of difference + 0x7fff is "grew", spread over the half
-        const unsigned up = prmt(nb - lb + 0x7FFF7FFFu, 0u, 0xBB99u);
+        // bit 15 of lb - nb per half is "grew", spread over the half
+        const unsigned up = prmt(__vsub2(lb, nb), 0u, 0xBB99u);
 #pragma unroll
         for (int u = 0; u < 4; ++u) sv[u] = (hk[u] & up) | (sv[u] & ~up);
         g_lo = (up & 1u) ? g0 : g_lo;
