@@ -184,11 +184,12 @@ __device__ __forceinline__ void chunk16(Cells16& c, const K16& K, const Grp<L>& 
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
         // Every operand half is a biased value >= pmax and every difference
-        // is taken between values known to be ordered, so the per-half adds
-        // and subtracts below never wrap.  They are written as 16x2 adds
-        // (__vadd2 / __vsub2), which issue on the FMA pipe: the DPX maxima,
-        // permutes and logic of the step all take the ALU pipe, which runs
-        // at half rate and bounds the step.
+        // is taken between values known to be ordered, so the adds and
+        // subtracts below never carry or borrow across halves.  They are
+        // written to issue on the FMA pipe: 16x2 adds of a constant, and
+        // multiply-adds by the run-time constants ONE / NEG1.  The DPX
+        // maxima, permutes and logic of the step all take the ALU pipe,
+        // which runs at half rate and bounds the step.
         const unsigned tp = prmt(tw, tpv, tsel(u));
         const unsigned mis = flag2(c.qp ^ tp);  // 0: match, 1: mismatch
         const unsigned diag = __vadd2(c.hd, K.MATCH2) - mis * K.MX;  // one multiply-add, no borrow
@@ -199,15 +200,17 @@ __device__ __forceinline__ void chunk16(Cells16& c, const K16& K, const Grp<L>& 
         unsigned E = __viaddmax_u16x2(c.el, K.NGE2, ea);
         unsigned H = umax2(M, E);
         if (TB) {
-            // Each flag is bit 15 of a half of (smaller - larger) of an
-            // ordered pair: set when their difference is at least 1.  The
-            // classifier keeps every difference within 15 bits, so a
-            // difference of d >= 1 leaves 2^16 - d >= 2^15 in the half.
-            const unsigned n1 = __vsub2(diag, H);  // H != diag
-            const unsigned n2 = __vsub2(F, H);     // H != F
-            const unsigned fc = __vsub2(fa, F);    // F extends (F above - ext > H above - open)
-            unsigned ec = 0u;                      // E extends
-            if (EM == 0) ec = __vsub2(ea, E);      //   open > ext: E_left - ext > M_left - open
+            // Each flag is bit 15 of a half of (ordered difference + 0x7fff):
+            // set when the difference is at least 1.  The classifier keeps
+            // every difference within 15 bits, so the sums neither carry nor
+            // borrow across halves (the 32-bit x + 0x7fff7fff may carry, and
+            // the subtraction that follows takes the carry back).
+            const unsigned hb = H * K.ONE + 0x7FFF7FFFu;
+            const unsigned n1 = diag * K.NEG1 + hb;                        // H != diag
+            const unsigned n2 = F * K.NEG1 + hb;                           // H != F
+            const unsigned fc = fa * K.NEG1 + (F * K.ONE + 0x7FFF7FFFu);   // F extends (F above - ext > H above - open)
+            unsigned ec = 0u;                                              // E extends
+            if (EM == 0) ec = ea * K.NEG1 + (E * K.ONE + 0x7FFF7FFFu);     //   open > ext: E_left - ext > M_left - open
             if (EM == 2) ec = c.el - E + K.EB2;          //   open < ext: E == E_left - ext (ties extend)
             // sign-replicated high bytes: [n1.lo n1.hi n2.lo n2.hi], [fc.lo fc.hi ec.lo ec.hi]
             const unsigned w1 = prmt(n1, n2, 0xFDB9u);
@@ -301,8 +304,8 @@ struct BestTrack16 {
     __device__ __forceinline__ void update(unsigned& lb, const unsigned (&hk)[4], int g0) {
         const unsigned nb = __vimax3_u16x2(lb, __vimax3_u16x2(hk[0], hk[1], hk[2]), hk[3]);
         // nb >= lb in each half and the difference stays within 15 bits:
-        // bit 15 of lb - nb per half is "grew", spread over the half
-        const unsigned up = prmt(__vsub2(lb, nb), 0u, 0xBB99u);
+        // bit 15 of difference + 0x7fff is "grew", spread over the half
+        const unsigned up = prmt(nb - lb + 0x7FFF7FFFu, 0u, 0xBB99u);
 #pragma unroll
         for (int u = 0; u < 4; ++u) sv[u] = (hk[u] & up) | (sv[u] & ~up);
         g_lo = (up & 1u) ? g0 : g_lo;

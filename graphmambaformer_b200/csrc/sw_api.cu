@@ -261,6 +261,8 @@ static void fill_args(SwArgs& a, const gmf_pairs* pairs, const gmf_sw_params* pa
     k.NGE2 = ((0x10000u - (unsigned)a.e16) & 0xFFFFu) * one2;
     k.MX = (unsigned)(a.m16 + a.x16);
     k.EB2 = (0x8000u - (unsigned)a.e16) * one2;
+    k.ONE = 1u;
+    k.NEG1 = 0xFFFFFFFFu;
     k.G = g;
     a.score = res->score;
     a.q_end = res->query_end;

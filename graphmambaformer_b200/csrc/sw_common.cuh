@@ -33,6 +33,9 @@ struct K16 {
     unsigned MX;                 // match + mismatch (a mismatch flag times this is subtracted)
     unsigned EB2;                // 0x8000 - extend (packed): bit 15 of E_left - E + EB2 is E == E_left - extend
     int G;                       // gcd of the scoring: true score = scaled score * G
+    // 1 and 2^32 - 1, read at run time: x * ONE + c and y * NEG1 + x are adds
+    // and subtracts the compiler must issue as multiply-adds (FMA pipe)
+    unsigned ONE, NEG1;
     __host__ __device__ unsigned init_pk() const { return Z | (NEGV << 16); }  // row 0: H = 0, F = -inf
 };
 
