@@ -134,7 +134,8 @@ struct TWin {
         wi = 0;
         tsh = 0;
     }
-    __device__ unsigned ld(int i) const { return __ldg(w32 + imin(imax(i, 0), nwords - 1)); }
+    // a negative index wraps to a large unsigned one and reads the last word
+    __device__ unsigned ld(int i) const { return __ldg(w32 + min((unsigned)i, (unsigned)(nwords - 1))); }
     __device__ void start(int code_index, bool active) {  // window at code index `code_index` of the pair
         const long long off = pair_t + (long long)code_index;
         tsh = (int)(off & 3) * 8;
@@ -301,16 +302,20 @@ struct BestTrack16 {
         sv[0] = sv[1] = sv[2] = sv[3] = z2;
         g_lo = g_hi = 0;
     }
+    // Run by the whole warp (every caller's chunk loop is warp-uniform): the
+    // selects are skipped in the chunks where no lane's maximum grows.
     __device__ __forceinline__ void update(unsigned& lb, const unsigned (&hk)[4], int g0) {
         const unsigned nb = __vimax3_u16x2(lb, __vimax3_u16x2(hk[0], hk[1], hk[2]), hk[3]);
-        // nb >= lb in each half and the difference stays within 15 bits:
-        // bit 15 of difference + 0x7fff is "grew", spread over the half
-        const unsigned up = prmt(nb - lb + 0x7FFF7FFFu, 0u, 0xBB99u);
+        if (__any_sync(FULL_MASK, nb != lb)) {
+            // nb >= lb in each half and the difference stays within 15 bits:
+            // bit 15 of difference + 0x7fff is "grew", spread over the half
+            const unsigned up = prmt(nb - lb + 0x7FFF7FFFu, 0u, 0xBB99u);
 #pragma unroll
-        for (int u = 0; u < 4; ++u) sv[u] = (hk[u] & up) | (sv[u] & ~up);
-        g_lo = (up & 1u) ? g0 : g_lo;
-        g_hi = (up >> 31) ? g0 : g_hi;
-        lb = nb;
+            for (int u = 0; u < 4; ++u) sv[u] = (hk[u] & up) | (sv[u] & ~up);
+            g_lo = (up & 1u) ? g0 : g_lo;
+            g_hi = (up >> 31) ? g0 : g_hi;
+            lb = nb;
+        }
     }
     // Global steps of the first cell of each half that holds its maximum.
     __device__ __forceinline__ void positions(unsigned lb, int& pos0, int& pos1) const {
