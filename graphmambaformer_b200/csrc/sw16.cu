@@ -406,7 +406,10 @@ __device__ void sw16_group(const SwArgs& a, int p, const Grp<L>& grp, uint32_t* 
 
     const int8_t* __restrict__ q = G.q;
     const int c0 = G.off - G.hb;  // j = row + c0 + d
-    int d = -4 * k;               // slot of the low half at the chunk start
+    int d = -4 * k;               // slot of the low half at the chunk start (x-drop bookkeeping)
+    int until = k;                // chunks until the lane's next row start (every P / 4 chunks)
+    int tbi = k;                  // word of the chunk's traceback bits: (g0 / 4) * L + k
+    const int tb_end = last_chunk * L + k;
     int row = 2 * k + 1 - V;      // row of the low half (advanced by V at each row start)
     Cells16 c;
     cells_init(c, K);
@@ -421,7 +424,8 @@ __device__ void sw16_group(const SwArgs& a, int p, const Grp<L>& grp, uint32_t* 
     const int dW0 = (W - 1) & ~3, dW1 = (W + 1) & ~3;  // chunks that end a row (x-drop)
 
     for (int g0 = 0; g0 <= loop_last; g0 += 4) {
-        if (d == 0) {  // both halves start new rows (the high half two steps later)
+        if (until == 0) {  // both halves start new rows (the high half two steps later)
+            until = P >> 2;
             row += V;
             row_start16(c, row, row + c0, qlen, tlen, W, q);
             tw.start(row + c0 - 1, active);
@@ -445,7 +449,8 @@ __device__ void sw16_group(const SwArgs& a, int p, const Grp<L>& grp, uint32_t* 
         // ---- once per chunk ----
         tpv = prmt(twin, tpv, 0x4344u);  // this chunk's last code, for the next chunk's high half
         tw.advance(active);
-        if (TB && (g0 >> 2) <= last_chunk) bits[(g0 >> 2) * L + k] = c.acc;
+        if (TB && tbi <= tb_end) bits[tbi] = c.acc;
+        tbi += L;
         if (use_ring && k == L - 1)
             *reinterpret_cast<uint4*>(ring + (g0 & rmask)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
         if (XD)
@@ -457,8 +462,11 @@ __device__ void sw16_group(const SwArgs& a, int p, const Grp<L>& grp, uint32_t* 
             if (d == dW1 && row + 1 <= qlen && row >= 1) rowmax[row] = make_int2((hi16(lb) - (int)K.Z) * K.G, pos1);
         }
         __syncwarp();
-        d += 4;
-        if (d == P) d = 0;
+        --until;
+        if (XD) {
+            d += 4;
+            if (d == P) d = 0;
+        }
     }
     __syncwarp();
 
@@ -613,7 +621,10 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* pro
     const int rmask = a.ring - 1;
     const unsigned INIT = K.init_pk();
 
-    int d = -4 * lane;  // slot of the low half at the chunk start
+    int d = -4 * lane;  // slot of the low half at the chunk start (x-drop bookkeeping)
+    int until = lane;   // chunks until the lane's next row start (every P / 4 chunks)
+    int tbi = 0x3fffffff;  // word of the chunk's traceback bits ((t + gofs) / 4 * L + lane), none before a row
+    const int tb_end = last_chunk * L + lane;
     int kk = -1;        // local index of the lane's current strip
     int row = 0, gofs = 0;
     Cells16 c;
@@ -628,11 +639,13 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* pro
 
     if (kk_last >= 0) {
         for (int t = 0; t < loop_end; t += 4) {
-            if (d == 0) {
+            if (until == 0) {
+                until = P >> 2;
                 ++kk;
                 const int s = w + NW * kk;
                 row = s * V + 2 * lane + 1;
                 gofs = (s - kk) * P;  // local step -> step of the one-warp schedule
+                tbi = ((t + gofs) >> 2) * L + lane;
                 row_start16(c, row, row + c0, qlen, tlen, W, q);
                 tw.start(row + c0 - 1, true);
                 tpv = 0u;
@@ -676,7 +689,8 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* pro
                 if (!a.coop_stall) st_release_cta(prog + w, t + 4);
             }
             const int g0 = t + gofs;
-            if (TB && kk >= 0 && (g0 >> 2) <= last_chunk) bits[(g0 >> 2) * L + lane] = c.acc;
+            if (TB && tbi <= tb_end) bits[tbi] = c.acc;
+            tbi += L;
             if (XD)
                 best16<XD>(lb, pos0, pos1, hk, g0, d);
             else
@@ -686,8 +700,11 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* pro
                 if (d == dW1 && row + 1 <= qlen) rowmax[row] = make_int2((hi16(lb) - (int)K.Z) * K.G, pos1);
             }
             __syncwarp();
-            d += 4;
-            if (d == P) d = 0;
+            --until;
+            if (XD) {
+                d += 4;
+                if (d == P) d = 0;
+            }
         }
     }
     __syncthreads();  // every traceback word and row maximum is written
