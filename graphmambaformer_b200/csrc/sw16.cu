@@ -12,10 +12,12 @@
 // only when smax + Z + 2*pmax + 64 <= 65535, so all cells are exact unsigned
 // 16-bit integers and the local-alignment floor is a three-way max with Z.
 // The step uses the DPX __viaddmax_u16x2 / __viaddmin_u16x2 / __vimax3_u16x2,
-// byte permutes, funnel shifts and plain 32-bit integer ops (packed adds and
-// subtracts that cannot carry across halves are 32-bit adds).  Comparisons are differences of values known
-// to be ordered (H >= M >= diag, H >= F, F >= fa, E >= ea, E >= eb), turned
-// into 0/1 flags with min(x, 1).
+// byte permutes and logic on the ALU pipe, and puts its adds on the FMA pipe
+// (16x2 adds of constants, multiply-adds): the ALU pipe issues at half rate
+// and bounds the step.  Packed adds and subtracts never carry or borrow
+// across halves.  Comparisons are differences of values known to be ordered
+// (H >= M >= diag, H >= F, F >= fa, E >= ea, E >= eb), read as bit 15 of
+// (difference + 0x7fff) per half.
 //
 // Layout: a pair is aligned by a group of L lanes (L = 8, 16 or 32, so one
 // warp aligns 4, 2 or 1 pairs).  Lane k carries two "virtual lanes", 2k in the
