@@ -425,12 +425,40 @@ __device__ void sw16_group(const SwArgs& a, int p, const Grp<L>& grp, uint32_t* 
     const bool from_rv = use_ring && k == 0;
     const int dW0 = (W - 1) & ~3, dW1 = (W + 1) & ~3;  // chunks that end a row (x-drop)
 
+    // The lane's next row (query codes, band counters, target window) is
+    // prepared by the whole group in the chunk where the group's lane 0
+    // starts its row (until == k there), and taken up k chunks later: the
+    // loads and bounds run once per period for all lanes instead of one lane
+    // at a time.
+    unsigned nqp = 0u, nma = 0u, nmb = 0u, nw0 = 0u, nw1 = 0u, nw2 = 0u;
+    int nwi = 0, ntsh = 0;
+
     for (int g0 = 0; g0 <= loop_last; g0 += 4) {
+        if (until == k) {
+            Cells16 nx;
+            row_start16(nx, row + V, row + V + c0, qlen, tlen, W, q);
+            TWin tn = tw;
+            tn.start(row + V + c0 - 1, active);
+            nqp = nx.qp;
+            nma = nx.ma;
+            nmb = nx.mb;
+            nw0 = tn.w0;
+            nw1 = tn.w1;
+            nw2 = tn.w2;
+            nwi = tn.wi;
+            ntsh = tn.tsh;
+        }
         if (until == 0) {  // both halves start new rows (the high half two steps later)
             until = P >> 2;
             row += V;
-            row_start16(c, row, row + c0, qlen, tlen, W, q);
-            tw.start(row + c0 - 1, active);
+            c.qp = nqp;
+            c.ma = nma;
+            c.mb = nmb;
+            tw.w0 = nw0;
+            tw.w1 = nw1;
+            tw.w2 = nw2;
+            tw.wi = nwi;
+            tw.tsh = ntsh;
             tpv = 0u;
             if (XD) {
                 lb = K.Z2;
@@ -639,8 +667,28 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* pro
     const int src = (lane + 31) & 31;
     const int dW0 = (W - 1) & ~3, dW1 = (W + 1) & ~3;
 
+    // the lane's next row, prepared by the whole warp when lane 0 starts its
+    // strip (until == lane there) and taken up lane chunks later
+    unsigned nqp = 0u, nma = 0u, nmb = 0u, nw0 = 0u, nw1 = 0u, nw2 = 0u;
+    int nwi = 0, ntsh = 0;
+
     if (kk_last >= 0) {
         for (int t = 0; t < loop_end; t += 4) {
+            if (until == lane) {
+                const int nrow = (w + NW * (kk + 1)) * V + 2 * lane + 1;
+                Cells16 nx;
+                row_start16(nx, nrow, nrow + c0, qlen, tlen, W, q);
+                TWin tn = tw;
+                tn.start(nrow + c0 - 1, true);
+                nqp = nx.qp;
+                nma = nx.ma;
+                nmb = nx.mb;
+                nw0 = tn.w0;
+                nw1 = tn.w1;
+                nw2 = tn.w2;
+                nwi = tn.wi;
+                ntsh = tn.tsh;
+            }
             if (until == 0) {
                 until = P >> 2;
                 ++kk;
@@ -648,8 +696,14 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* pro
                 row = s * V + 2 * lane + 1;
                 gofs = (s - kk) * P;  // local step -> step of the one-warp schedule
                 tbi = ((t + gofs) >> 2) * L + lane;
-                row_start16(c, row, row + c0, qlen, tlen, W, q);
-                tw.start(row + c0 - 1, true);
+                c.qp = nqp;
+                c.ma = nma;
+                c.mb = nmb;
+                tw.w0 = nw0;
+                tw.w1 = nw1;
+                tw.w2 = nw2;
+                tw.wi = nwi;
+                tw.tsh = ntsh;
                 tpv = 0u;
                 if (XD) {
                     lb = K.Z2;
