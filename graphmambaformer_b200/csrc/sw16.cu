@@ -605,9 +605,17 @@ __device__ __forceinline__ void st_release_cta(int* p, int v) {
 }
 
 template <int NW, bool TB, bool XD, int EM>
-__device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* prog, int (*sbest)[3],
+__device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* prog, int* cons, int (*sbest)[3],
                                uint32_t** sws) {
     constexpr int L = 32, V = 64;
+    // The 8-warp class (wide bands) bounds each warp's lead over the warp that
+    // reads it as well: lane 31 waits until its reader has taken the entries
+    // it is about to overwrite, so a ring of a.ring entries (1024) serves
+    // periods up to COOP_PMAX instead of needing P + 8.  A warp's lag behind
+    // its predecessor then stays within [132, a.ring + 128] steps; the lags
+    // of the NW links sum to P, so with NW * 132 <= P <= NW * (a.ring + 128)
+    // the warps cannot all be waiting at once.
+    constexpr bool BP = NW == 8;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     Grp<32> grp(lane);
     PairGeo G = load_geo(a, p);
@@ -628,7 +636,10 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* pro
         uint32_t* ws0 = ws_alloc<32>(a, grp, tbw + (XD ? 2ull * qlen : 0ull), TB || XD);
         if (lane == 0) *sws = ws0;
     }
-    if (threadIdx.x < NW) prog[threadIdx.x] = 0;
+    if (threadIdx.x < NW) {
+        prog[threadIdx.x] = 0;
+        cons[threadIdx.x] = (int)threadIdx.x < nstrips ? 0 : 0x7fffffff;  // a warp without strips reads nothing
+    }
     __syncthreads();
     uint32_t* ws = *sws;
     if ((TB || XD) && !ws) {
@@ -734,6 +745,9 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* pro
                 } else {
                     rv[0] = rv[1] = rv[2] = rv[3] = INIT;  // row 0, or a strip past the query
                 }
+                // the previous warp's entries before t + 4 * L (+ 4), in its step
+                // numbering, are no longer needed (also when this strip reads none)
+                if (BP) st_release_cta(cons + w, t + 4 * L + 4 - (w == 0 ? P : 0));
             }
             const unsigned twin = tw.window();
             unsigned hk[4], pk[4];
@@ -741,6 +755,19 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* pro
             tpv = prmt(twin, tpv, 0x4344u);
             tw.advance(true);
             if (lane == 31) {  // publish before the global store, so the release does not wait on it
+                if (BP) {
+                    // the slots of steps t .. t+3 held steps t - ring .. t - ring + 3
+                    const int need = t + 4 - a.ring;
+                    int spins = 0;
+                    while (ld_acquire_cta(cons + (w + 1) % NW) < need) {
+                        if (++spins > a.coop_spin_limit ||
+                            ((spins & 1023) == 0 && (*(volatile int*)a.err & (int)GMF_SWF_TIMEOUT))) {
+                            atomicOr(a.err, (int)GMF_SWF_TIMEOUT);
+                            break;
+                        }
+                        __nanosleep(20);
+                    }
+                }
                 *reinterpret_cast<uint4*>(ring_out + (t & rmask)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
                 if (!a.coop_stall) st_release_cta(prog + w, t + 4);
             }
@@ -763,6 +790,7 @@ __device__ void sw16_coop_pair(const SwArgs& a, int p, uint32_t* rings, int* pro
             }
         }
     }
+    if (BP && lane == 0 && kk_last >= 0) st_release_cta(cons + w, 0x7fffffff);  // reads nothing more
     __syncthreads();  // every traceback word and row maximum is written
 
     int bh = 0, bi = 0, bd = 0;
@@ -830,6 +858,7 @@ __global__ void __launch_bounds__(32 * NW) sw16_coop_kernel(SwArgs a) {
     extern __shared__ uint4 coop_ring4[];
     uint32_t* rings = reinterpret_cast<uint32_t*>(coop_ring4);
     __shared__ int prog[NW];
+    __shared__ int cons[NW];
     __shared__ int sbest[NW][3];
     __shared__ uint32_t* sws;
     __shared__ int spair;
@@ -841,7 +870,7 @@ __global__ void __launch_bounds__(32 * NW) sw16_coop_kernel(SwArgs a) {
         __syncthreads();
         const int idx = spair;
         if (idx >= count) break;
-        sw16_coop_pair<NW, TB, XD, EM>(a, list[idx], rings, prog, sbest, &sws);
+        sw16_coop_pair<NW, TB, XD, EM>(a, list[idx], rings, prog, cons, sbest, &sws);
         __syncthreads();
     }
 }

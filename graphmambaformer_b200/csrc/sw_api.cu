@@ -502,7 +502,9 @@ extern "C" int gmf_banded_sw(const gmf_pairs* pairs, const gmf_sw_params* params
     for (int c = 0; c < 3; ++c) {
         if (Pmax < coop_pmin[c] || tun.coop_min_strips[coop_knob[c]] <= 0) continue;  // class empty
         SwArgs ac = a;
-        ac.ring = ring_entries(std::min(Pmax, coop_pcap[c]) + 7);
+        // the 8-warp class bounds each warp's lead over its reader (1024 entries
+        // cover periods up to COOP_PMAX); the others hold a whole period
+        ac.ring = coop_cls[c] == CLS_I16_C8 ? 1024 : ring_entries(std::min(Pmax, coop_pcap[c]) + 7);
         if ((size_t)sw16_coop_warps(coop_cls[c]) * ac.ring * 4 > (size_t)di.smem_optin) return GMF_ERR_LIMIT;
         cudaStream_t s;
         GMF_TRY(next_stream(&s));
