@@ -580,11 +580,13 @@ __global__ void __launch_bounds__(128) sw16_kernel(SwArgs a) {
 // runs at least 4L + 4 steps behind its predecessor, and the cycle of NW
 // warps keeps moving only when P >= NW * (4L + 4) -- the classifier sends a
 // pair here only then.  Under that bound no writer is ever more than P
-// entries ahead of its reader, so a ring of R >= P + 8 entries needs no
-// back-pressure.  Each writer publishes its progress after every chunk (ring
-// store, then a release store of the flag); each reader polls the flag with
-// acquire loads and an iteration limit, after which it records
-// GMF_SWF_TIMEOUT and goes on.
+// entries ahead of its reader, so the 2- and 4-warp classes use rings of
+// R >= P + 8 entries and no back-pressure.  The 8-warp class (periods up to
+// COOP_PMAX) adds back-pressure instead and keeps 1,024-entry rings: its
+// writers also wait for their readers (see sw16_coop_pair).  Each writer
+// publishes its progress after every chunk (ring store, then a release store
+// of the flag); each reader polls the flag with acquire loads and an
+// iteration limit, after which it records GMF_SWF_TIMEOUT and goes on.
 // Traceback words land at the same (global step, lane) positions as in the
 // one-warp layout, so the walk (warp 0, after a block barrier) is unchanged.
 // ---------------------------------------------------------------------------

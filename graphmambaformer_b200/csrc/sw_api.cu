@@ -493,8 +493,9 @@ extern "C" int gmf_banded_sw(const gmf_pairs* pairs, const gmf_sw_params* params
         *out = ss->s[used++];
         return GMF_OK;
     };
-    // cooperative classes, each with a ring of P + 8 entries per warp for the
-    // largest period the class can hold
+    // cooperative classes: the 2- and 4-warp ones with a ring of P + 8 entries
+    // per warp for the largest period the class can hold, the 8-warp one with
+    // back-pressure and a fixed ring
     const int coop_cls[3] = {CLS_I16_C8, CLS_I16_C4, CLS_I16_C2};
     const int coop_pmin[3] = {8 * 132, 4 * 132, 2 * 132};
     const int coop_pcap[3] = {COOP_PMAX, 8 * 132 - 4, 4 * 132 - 4};
