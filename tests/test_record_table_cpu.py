@@ -187,3 +187,18 @@ def test_sam_batch_of_hand_made_records_equals_object_path():
             want = sam_records(results, seqs, "illumina", secondary, refs)
             got = sam_batch(table, ["a", "b", "c"], ascii_, s_off, None, "illumina", secondary, refs)
             _same_layout(got, want)
+
+
+def test_record_table_from_extension_objects_equals_object_path():
+    """The WFA path's batches hold ready ExtensionResults instead of columns;
+    record_table reads those the same way."""
+    from graphmambaformer_b200.types import ExtensionResult
+
+    rng = np.random.default_rng(6)
+    cols_batch = _synthetic_batch(rng, R=25)
+    objs = [cols_batch._chain(c) for c in range(int(cols_batch.chain_off[-1]))]
+    assert all(isinstance(e, ExtensionResult) for e in objs)
+    obj_batch = BatchAlignments(cols_batch.n_reads, cols_batch.chain_off, objects=objs, chains=cols_batch.chains)
+    a, b = record_table(cols_batch), record_table(obj_batch)
+    for f in fields(a):
+        assert np.array_equal(getattr(a, f.name), getattr(b, f.name)), f.name
